@@ -1,0 +1,348 @@
+"""curplsh_b200 -- B200-native exact L2 k-nearest-neighbour engine.
+
+Python mirror of cuRPLSH's host interface (``Index`` / ``IndexBF`` /
+``DeviceResources``, include/index.h, include/index_bf.h,
+include/device_resources.h), bound with ctypes to the C ABI of
+``libcurplsh_b200.so`` (include/curplsh_b200.h).  The compute path is the
+CUDA library; if it is missing this module raises on import -- there is no
+CPU fallback.
+
+Arrays may be numpy arrays (host memory) or torch tensors (host or CUDA);
+float32, C-contiguous.  Methods named like the reference take the same
+arguments (``add(num, data)``, ``search(num, queries, k, indices,
+distances)``); ``add_array`` / ``search_array`` are the convenience forms
+returning new arrays.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = [
+    "DeviceResources", "IndexBF", "IndexBFConfig", "MemorySpace", "Precision", "CurplshError",
+    "compute_l2_norm", "search_l2_distance", "lib_path", "get_num_devices",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libcurplsh_b200.so")
+
+
+class CurplshError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"curplsh error {code}: {msg}")
+        self.code = code
+
+
+OK, ERR_INVALID_ARG, ERR_CUDA, ERR_OOM, ERR_UNSUPPORTED, ERR_DEVICE, ERR_STATE = range(7)
+
+
+class MemorySpace:
+    """include/memory_space.h:12-17"""
+    Device = 0
+    Unified = 1
+
+
+class Precision:
+    FP32_EXACT = 0
+    BF16_RERANK = 1
+    FP8_RERANK = 2
+
+
+class _Cfg(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("memory_space", ctypes.c_int32),
+                ("store_transposed", ctypes.c_int32), ("compute_exact_distances", ctypes.c_int32),
+                ("precision", ctypes.c_int32), ("rerank_factor", ctypes.c_int32),
+                ("borrow_device_data", ctypes.c_int32)]
+
+
+def lib_path() -> str:
+    return _LIB_PATH
+
+
+def _load():
+    if not os.path.exists(_LIB_PATH):
+        raise ImportError(f"{_LIB_PATH} is missing: run `python -m curplsh_b200.build` "
+                          "(there is no CPU fallback)")
+    lib = ctypes.CDLL(_LIB_PATH)
+    vp, i32, i64, f32p, i32p = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p
+    sig = {
+        "curplsh_bf_config_init": (None, [ctypes.POINTER(_Cfg)]),
+        "curplsh_last_error": (ctypes.c_char_p, []),
+        "curplsh_version": (ctypes.c_char_p, []),
+        "curplsh_get_num_devices": (i32, [ctypes.POINTER(ctypes.c_int)]),
+        "curplsh_resources_create": (i32, [ctypes.POINTER(vp)]),
+        "curplsh_resources_destroy": (i32, [vp]),
+        "curplsh_resources_initialize_for_device": (i32, [vp, i32]),
+        "curplsh_resources_get_default_stream": (i32, [vp, i32, ctypes.POINTER(vp)]),
+        "curplsh_resources_set_default_stream": (i32, [vp, i32, vp]),
+        "curplsh_resources_get_alternate_streams": (i32, [vp, i32, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_int)]),
+        "curplsh_resources_get_async_copy_stream": (i32, [vp, i32, ctypes.POINTER(vp)]),
+        "curplsh_resources_sync_default_stream": (i32, [vp, i32]),
+        "curplsh_index_bf_create": (i32, [vp, i32, ctypes.POINTER(_Cfg), ctypes.POINTER(vp)]),
+        "curplsh_index_destroy": (i32, [vp]),
+        "curplsh_index_train": (i32, [vp, i64, f32p]),
+        "curplsh_index_add": (i32, [vp, i64, f32p]),
+        "curplsh_index_search": (i32, [vp, i64, f32p, i32, i32p, f32p]),
+        "curplsh_index_search_ex": (i32, [vp, i64, f32p, i32, i32, i32, i32p, f32p, vp]),
+        "curplsh_index_search_profiled": (i32, [vp, i64, f32p, i32, i32, i32, i32p, f32p, vp,
+                                                ctypes.POINTER(ctypes.c_float)]),
+        "curplsh_index_reset": (i32, [vp]),
+        "curplsh_index_get_dimension": (i32, [vp, ctypes.POINTER(ctypes.c_int)]),
+        "curplsh_index_get_num_data": (i32, [vp, ctypes.POINTER(ctypes.c_int64)]),
+        "curplsh_index_get_device": (i32, [vp, ctypes.POINTER(ctypes.c_int)]),
+        "curplsh_compute_l2_norm": (i32, [f32p, i64, i32, f32p, i32, vp]),
+        "curplsh_search_l2_distance": (i32, [vp, f32p, i64, f32p, f32p, i64, i32, i32, i32p, f32p, i32]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+_lib = _load()
+
+# Every symbol the C header declares; tests check the library exports them all.
+EXPORTED_SYMBOLS = (
+    "curplsh_bf_config_init", "curplsh_last_error", "curplsh_version", "curplsh_get_num_devices",
+    "curplsh_resources_create", "curplsh_resources_destroy", "curplsh_resources_initialize_for_device",
+    "curplsh_resources_get_default_stream", "curplsh_resources_set_default_stream",
+    "curplsh_resources_get_alternate_streams", "curplsh_resources_get_async_copy_stream",
+    "curplsh_resources_sync_default_stream", "curplsh_index_bf_create", "curplsh_index_destroy",
+    "curplsh_index_train", "curplsh_index_add", "curplsh_index_search", "curplsh_index_search_ex",
+    "curplsh_index_search_profiled", "curplsh_index_reset", "curplsh_index_get_dimension",
+    "curplsh_index_get_num_data", "curplsh_index_get_device", "curplsh_compute_l2_norm",
+    "curplsh_search_l2_distance",
+)
+
+
+def _check(rc: int):
+    if rc != OK:
+        raise CurplshError(rc, _lib.curplsh_last_error().decode(errors="replace"))
+
+
+def version() -> str:
+    return _lib.curplsh_version().decode()
+
+
+def get_num_devices() -> int:
+    n = ctypes.c_int(0)
+    _check(_lib.curplsh_get_num_devices(ctypes.byref(n)))
+    return n.value
+
+
+# ------------------------------------------------------------------ arrays
+def _ptr(a, dtype, writable=False):
+    """Raw pointer of a float32/int32 C-contiguous numpy array or torch tensor."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr") and hasattr(a, "is_contiguous"):  # torch tensor
+        import torch
+        want = {np.float32: torch.float32, np.int32: torch.int32}[dtype]
+        if a.dtype != want or not a.is_contiguous():
+            raise TypeError(f"expected a contiguous {want} tensor")
+        return ctypes.c_void_p(a.data_ptr())
+    if not isinstance(a, np.ndarray):
+        raise TypeError("expected a numpy array or torch tensor")
+    if a.dtype != dtype or not a.flags.c_contiguous or (writable and not a.flags.writeable):
+        raise TypeError(f"expected a C-contiguous {np.dtype(dtype)} array")
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        return None
+    if hasattr(stream, "cuda_stream"):
+        return ctypes.c_void_p(stream.cuda_stream)
+    return ctypes.c_void_p(int(stream))
+
+
+# ------------------------------------------------------------------ resources
+class DeviceResources:
+    """include/device_resources.h:60-263 (streams per device; no cuBLAS/cuRAND handles are needed)."""
+
+    def __init__(self, devices=None):
+        h = ctypes.c_void_p()
+        _check(_lib.curplsh_resources_create(ctypes.byref(h)))
+        self._h = h
+        if devices is not None:
+            for d in ([devices] if isinstance(devices, int) else devices):
+                self.initializeForDevice(d)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.curplsh_resources_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def initializeForDevice(self, device: int):
+        _check(_lib.curplsh_resources_initialize_for_device(self._h, device))
+
+    def getDefaultStream(self, device: int) -> int:
+        s = ctypes.c_void_p()
+        _check(_lib.curplsh_resources_get_default_stream(self._h, device, ctypes.byref(s)))
+        return s.value or 0
+
+    def setDefaultStream(self, device: int, stream) -> None:
+        _check(_lib.curplsh_resources_set_default_stream(self._h, device, _stream_ptr(stream)))
+
+    def getAlternateStreams(self, device: int):
+        arr = (ctypes.c_void_p * 2)()
+        n = ctypes.c_int(2)
+        _check(_lib.curplsh_resources_get_alternate_streams(self._h, device, arr, ctypes.byref(n)))
+        return [arr[i] or 0 for i in range(n.value)]
+
+    def getAsyncCopyStream(self, device: int) -> int:
+        s = ctypes.c_void_p()
+        _check(_lib.curplsh_resources_get_async_copy_stream(self._h, device, ctypes.byref(s)))
+        return s.value or 0
+
+    def syncDefaultStream(self, device: int) -> None:
+        _check(_lib.curplsh_resources_sync_default_stream(self._h, device))
+
+
+class IndexBFConfig:
+    """IndexBFConfig (include/index_bf.h:8-19) + IndexConfig (include/index.h:8-16) + precision controls."""
+
+    def __init__(self, device=0, memorySpace=MemorySpace.Device, storeTransposed=False,
+                 computeExactDistances=False, precision=Precision.FP32_EXACT, rerankFactor=4,
+                 borrowDeviceData=False):
+        self.device = device
+        self.memorySpace = memorySpace
+        self.storeTransposed = storeTransposed
+        self.computeExactDistances = computeExactDistances
+        self.precision = precision
+        self.rerankFactor = rerankFactor
+        self.borrowDeviceData = borrowDeviceData
+
+    def _c(self) -> _Cfg:
+        c = _Cfg()
+        _lib.curplsh_bf_config_init(ctypes.byref(c))
+        c.device = self.device
+        c.memory_space = self.memorySpace
+        c.store_transposed = int(bool(self.storeTransposed))
+        c.compute_exact_distances = int(bool(self.computeExactDistances))
+        c.precision = self.precision
+        c.rerank_factor = self.rerankFactor
+        c.borrow_device_data = int(bool(self.borrowDeviceData))
+        return c
+
+
+class IndexBF:
+    """Brute-force exact L2 index (include/index_bf.h:21-46, src/index_bf.cpp)."""
+
+    def __init__(self, resources: DeviceResources, dim: int, config: IndexBFConfig | None = None):
+        self._res = resources
+        self.config = config or IndexBFConfig()
+        h = ctypes.c_void_p()
+        cfg = self.config._c()
+        _check(_lib.curplsh_index_bf_create(resources._h, int(dim), ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self._keep = None  # borrowed device rows must outlive the index
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.curplsh_index_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- reference-shaped methods (include/index.h:29-64)
+    def train(self, num: int, data) -> None:
+        _check(_lib.curplsh_index_train(self._h, int(num), _ptr(data, np.float32) if data is not None else None))
+
+    def add(self, num: int, data) -> None:
+        if self.config.borrowDeviceData:
+            self._keep = data
+        _check(_lib.curplsh_index_add(self._h, int(num), _ptr(data, np.float32)))
+
+    def search(self, num: int, queries, k: int, indices, distances) -> None:
+        _check(_lib.curplsh_index_search(self._h, int(num), _ptr(queries, np.float32), int(k),
+                                         _ptr(indices, np.int32, True), _ptr(distances, np.float32, True)))
+
+    def search_ex(self, num: int, queries, k: int, indices, distances, precision: int = -1,
+                  rerank_factor: int = -1, stream=None) -> None:
+        _check(_lib.curplsh_index_search_ex(self._h, int(num), _ptr(queries, np.float32), int(k), int(precision),
+                                            int(rerank_factor), _ptr(indices, np.int32, True),
+                                            _ptr(distances, np.float32, True), _stream_ptr(stream)))
+
+    def search_profiled(self, num: int, queries, k: int, indices, distances, precision: int = -1,
+                        rerank_factor: int = -1, stream=None):
+        ms = (ctypes.c_float * 4)()
+        _check(_lib.curplsh_index_search_profiled(self._h, int(num), _ptr(queries, np.float32), int(k),
+                                                  int(precision), int(rerank_factor),
+                                                  _ptr(indices, np.int32, True), _ptr(distances, np.float32, True),
+                                                  _stream_ptr(stream), ms))
+        return {"prep_ms": ms[0], "fused_ms": ms[1], "merge_ms": ms[2], "total_ms": ms[3]}
+
+    def reset(self) -> None:
+        _check(_lib.curplsh_index_reset(self._h))
+        self._keep = None
+
+    def getDimension(self) -> int:
+        v = ctypes.c_int()
+        _check(_lib.curplsh_index_get_dimension(self._h, ctypes.byref(v)))
+        return v.value
+
+    def getNumData(self) -> int:
+        v = ctypes.c_int64()
+        _check(_lib.curplsh_index_get_num_data(self._h, ctypes.byref(v)))
+        return v.value
+
+    def getDevice(self) -> int:
+        v = ctypes.c_int()
+        _check(_lib.curplsh_index_get_device(self._h, ctypes.byref(v)))
+        return v.value
+
+    def getResources(self) -> DeviceResources:
+        return self._res
+
+    # -- convenience forms
+    def add_array(self, data) -> None:
+        self.add(int(data.shape[0]), data)
+
+    def search_array(self, queries, k: int, precision: int = -1, rerank_factor: int = -1):
+        """Returns (distances [nq,k] float32, indices [nq,k] int32) in the queries' memory space."""
+        nq = int(queries.shape[0])
+        if hasattr(queries, "is_cuda"):
+            import torch
+            dist = torch.empty((nq, k), dtype=torch.float32, device=queries.device)
+            idx = torch.empty((nq, k), dtype=torch.int32, device=queries.device)
+        else:
+            dist = np.empty((nq, k), dtype=np.float32)
+            idx = np.empty((nq, k), dtype=np.int32)
+        if precision < 0 and rerank_factor < 0:
+            self.search(nq, queries, k, idx, dist)
+        else:
+            self.search_ex(nq, queries, k, idx, dist, precision, rerank_factor)
+            if hasattr(queries, "is_cuda") and queries.is_cuda:
+                import torch
+                torch.cuda.synchronize(queries.device)
+        return dist, idx
+
+
+def compute_l2_norm(vectors, norms, squared: bool = True, stream=None) -> None:
+    """computeL2Norm (include/internal/norm.h:7-8) over device tensors."""
+    _check(_lib.curplsh_compute_l2_norm(_ptr(vectors, np.float32), int(vectors.shape[0]), int(vectors.shape[1]),
+                                        _ptr(norms, np.float32, True), int(bool(squared)), _stream_ptr(stream)))
+
+
+def search_l2_distance(resources: DeviceResources, bases, base_norms, queries, k: int, indices, distances,
+                       exact_distances: bool) -> None:
+    """searchL2Distance (include/internal/search.h:7-11) over device tensors."""
+    _check(_lib.curplsh_search_l2_distance(resources._h, _ptr(bases, np.float32), int(bases.shape[0]),
+                                           _ptr(base_norms, np.float32) if base_norms is not None else None,
+                                           _ptr(queries, np.float32), int(queries.shape[0]), int(queries.shape[1]),
+                                           int(k), _ptr(indices, np.int32, True), _ptr(distances, np.float32, True),
+                                           int(bool(exact_distances))))

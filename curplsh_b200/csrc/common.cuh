@@ -1,0 +1,111 @@
+// common.cuh -- definitions shared by the kernels and the host orchestration.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
+
+namespace curplsh_b200 {
+
+// ------------------------------------------------------------ precision forms
+// Form of the coarse (tensor-core) distance pass.  Every form finishes with
+// an exact FP32 rerank of its candidates, so returned distances are
+// sum_i (q_i - x_i)^2 in FP32 regardless of the coarse precision.
+enum Form : int {
+  kFormExact = 0,  // 3 x BF16 split products (hi*hi + hi*lo + lo*hi), FP32 accumulate
+  kFormBF16 = 1,   // BF16 x BF16, FP32 accumulate, k' = rerank_factor * k candidates
+  kFormFP8 = 2,    // FP8-E4M3 with per-vector FP32 scales, k' = rerank_factor * k
+};
+
+// ------------------------------------------------------------ device error word
+// Bit flags written (atomicOr) to a device status word by kernels that give up.
+enum DeviceError : uint32_t {
+  kErrNone = 0,
+  kErrWaitTimeout = 1u << 0,    // an mbarrier wait exceeded its poll limit
+  kErrPoolOverflow = 1u << 1,   // a candidate pool would have overflowed (never expected)
+  kErrBadSchedule = 1u << 2,    // unit bookkeeping out of range (never expected)
+};
+
+// ------------------------------------------------------------ ordered keys
+// Candidates are 64-bit keys: (order-preserving bits of the FP32 distance) << 32
+// | database row.  Unsigned comparison of keys is (distance, index)
+// lexicographic order, the engine's tie rule (lower index first).
+__host__ __device__ __forceinline__ uint32_t f_bits(float f) {
+#ifdef __CUDA_ARCH__
+  return __float_as_uint(f);
+#else
+  uint32_t u;
+  __builtin_memcpy(&u, &f, 4);
+  return u;
+#endif
+}
+__host__ __device__ __forceinline__ float bits_f(uint32_t u) {
+#ifdef __CUDA_ARCH__
+  return __uint_as_float(u);
+#else
+  float f;
+  __builtin_memcpy(&f, &u, 4);
+  return f;
+#endif
+}
+__host__ __device__ __forceinline__ uint32_t f2ord(float f) {
+  uint32_t u = f_bits(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__host__ __device__ __forceinline__ float ord2f(uint32_t o) {
+  uint32_t u = (o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o;
+  return bits_f(u);
+}
+__host__ __device__ __forceinline__ uint64_t make_key(float d, uint32_t idx) {
+  return ((uint64_t)f2ord(d) << 32) | idx;
+}
+constexpr uint64_t kKeyEmpty = ~0ull;
+constexpr uint32_t kOrdInf = 0xFFFFFFFFu;  // "no bound yet" for per-query thresholds
+
+// ------------------------------------------------------------ fused pass geometry
+constexpr int kBM = 128;          // queries per block: MMA M, one TMEM lane per query
+constexpr int kBN = 256;          // database rows per tile: MMA N (TMEM columns per accumulator)
+constexpr int kHalfN = kBN / 2;   // columns of a tile handled by one epilogue warpgroup
+constexpr int kChunkBytes = 128;  // K extent of one smem chunk row (one 128-byte swizzle atom)
+constexpr int kNumThreads = 320;  // warp 0 TMA producer, warp 1 MMA issuer, warps 2..9 epilogue
+constexpr int kEpiWarps = 8;
+
+struct FusedParams {
+  // problem
+  int nq;           // real number of queries
+  int nb;           // real number of database rows
+  int d;            // dimension
+  int kprime;       // candidates kept per query (before the FP32 rerank)
+  int pool_cap;     // capacity of one candidate pool (entries)
+  int form;         // Form
+  // schedule: flattened (query block, tile) space split evenly across CTAs
+  int num_qblocks;  // G
+  int num_tiles;    // T
+  long long work_per_cta;  // W
+  int units_per_block;     // U: max CTAs (units) that share one query block
+  // inputs
+  const float* db_norms;   // [nb_pad] squared norms, +inf for padding rows
+  const float* db_scale;   // [nb_pad] fp8 per-vector scales (FP8 form)
+  const float* q_norms;    // [nq_pad]
+  const float* q_scale;    // [nq_pad] (FP8 form)
+  // outputs / scratch
+  uint64_t* pools;         // [G*128][U][2][pool_cap]
+  int* pool_counts;        // [G*128][U][2]
+  uint32_t* q_bound;       // [nq_pad] shared per-query bound (ordered bits), init kOrdInf
+  uint32_t* status;        // device error word
+};
+
+struct MergeParams {
+  int nq, nb, d, k, kprime, pool_cap, units_per_block;
+  const uint64_t* pools;
+  const int* pool_counts;
+  const float* queries;    // [nq x d] fp32
+  const float* db;         // [nb x d] fp32 (row stride ld_db)
+  long long ld_db;
+  const uint32_t* q_bound;
+  int* out_idx;            // [nq x k]
+  float* out_dist;         // [nq x k]
+  uint32_t* status;
+};
+
+}  // namespace curplsh_b200

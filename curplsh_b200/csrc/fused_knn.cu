@@ -1,0 +1,573 @@
+// fused_knn.cu -- the fused distance + candidate-filter pass on the 5th-gen
+// tensor cores (sm_100a).
+//
+// Replaces, in one kernel, the reference's per-tile chain (cuRPLSH paths):
+//   matrixMultiply / cublasSgemm        src/internal/matrix_ops.cu:8-60   (-2 q.x)
+//   l2Select (+ ||x||^2, top-k)         src/internal/select.cu:189-224
+//   adjustIndices                       src/internal/search.cu:21-42      (tile -> global row)
+// The Q x N distance matrix never leaves the SM: each 128-query x 256-row
+// tile is accumulated in TMEM, read back by the epilogue warps, compared with a
+// per-query bound and only the survivors are appended to a per-query candidate
+// pool in global memory.
+//
+// Roles (320 threads, one CTA per SM, persistent over a balanced schedule):
+//   warp 0      TMA producer: query block (resident, or streamed per K chunk)
+//               and database tiles, 128-byte-swizzled, into a stage ring.
+//   warp 1      allocates 512 TMEM columns (two 128x256 f32 accumulators) and,
+//               from one lane, issues tcgen05.mma; commits release stages and
+//               publish accumulators.
+//   warps 2..9  epilogue: two warpgroups, each owning one 128-column half of
+//               every tile; thread = one query (TMEM lane).  A thread keeps its
+//               own pool and bound; a warp refreshes (radix-selects) a pool that
+//               is about to overflow, keeping the k' smallest (distance, row)
+//               keys, and publishes the tightened bound to the shared per-query
+//               bound array so other CTAs working on the same queries filter
+//               harder.
+//
+// Schedule: the (query block, database tile) space is flattened and split into
+// equal contiguous ranges, one per CTA, so the work is balanced to one tile for
+// any Q, N.  A range covers a few "units" = (query block, tile sub-range).
+#include <cuda.h>
+
+#include <cstdio>
+
+#include "common.cuh"
+#include "fused_knn.h"
+#include "ptx.cuh"
+#include "select.cuh"
+
+namespace curplsh_b200 {
+
+// ------------------------------------------------------------------ forms
+template <int FORM>
+struct FormTraits;
+template <>
+struct FormTraits<kFormExact> {
+  static constexpr int kAParts = 2, kBParts = 2, kProducts = 3;
+  static constexpr int kChunkElems = 64, kStepElems = 16;  // bf16
+  static constexpr bool kFP8 = false;
+  // products: hi*hi, hi*lo, lo*hi  (the lo*lo term, O(2^-16) relative, is dropped)
+  __device__ static constexpr int a_part(int p) { return p == 2 ? 1 : 0; }
+  __device__ static constexpr int b_part(int p) { return p == 1 ? 1 : 0; }
+};
+template <>
+struct FormTraits<kFormBF16> {
+  static constexpr int kAParts = 1, kBParts = 1, kProducts = 1;
+  static constexpr int kChunkElems = 64, kStepElems = 16;
+  static constexpr bool kFP8 = false;
+  __device__ static constexpr int a_part(int) { return 0; }
+  __device__ static constexpr int b_part(int) { return 0; }
+};
+template <>
+struct FormTraits<kFormFP8> {
+  static constexpr int kAParts = 1, kBParts = 1, kProducts = 1;
+  static constexpr int kChunkElems = 128, kStepElems = 32;  // e4m3
+  static constexpr bool kFP8 = true;
+  __device__ static constexpr int a_part(int) { return 0; }
+  __device__ static constexpr int b_part(int) { return 0; }
+};
+
+constexpr uint32_t kAChunkBytes = kBM * kChunkBytes;  // 16 KB
+constexpr uint32_t kBChunkBytes = kBN * kChunkBytes;  // 32 KB
+
+// ------------------------------------------------------------------ smem layout
+struct SmemLayout {
+  int nkc;             // K chunks (128 bytes of K each)
+  int a_stream;        // 1: query chunks travel with each stage
+  uint32_t a_bytes;    // resident query block bytes (0 when streamed)
+  uint32_t stage_bytes;
+  int stages;
+  uint32_t bar_off;    // offset of the barrier block
+  uint32_t hist_off;   // warp-private radix histograms
+  uint32_t total;      // dynamic smem bytes requested (includes 1 KB alignment slack)
+};
+
+__host__ __device__ inline SmemLayout make_layout(int form, int d) {
+  SmemLayout L{};
+  const int chunk_elems = (form == kFormFP8) ? 128 : 64;
+  const int a_parts = (form == kFormExact) ? 2 : 1;
+  const int b_parts = (form == kFormExact) ? 2 : 1;
+  L.nkc = (d + chunk_elems - 1) / chunk_elems;
+  const uint32_t budget = 200u * 1024u;
+  const uint32_t a_res = (uint32_t)L.nkc * a_parts * kAChunkBytes;
+  const uint32_t b_stage = (uint32_t)b_parts * kBChunkBytes;
+  if (a_res + 2 * b_stage <= budget) {
+    L.a_stream = 0;
+    L.a_bytes = a_res;
+    L.stage_bytes = b_stage;
+  } else {
+    L.a_stream = 1;
+    L.a_bytes = 0;
+    L.stage_bytes = b_stage + (uint32_t)a_parts * kAChunkBytes;
+  }
+  int s = (int)((budget - L.a_bytes) / L.stage_bytes);
+  L.stages = s < 2 ? 2 : (s > 8 ? 8 : s);
+  L.bar_off = L.a_bytes + (uint32_t)L.stages * L.stage_bytes;
+  L.hist_off = L.bar_off + 256;  // barriers: 2*8 + 6 mbarriers + tmem slot + flags < 256 B
+  L.total = L.hist_off + kEpiWarps * 256 * 4 + 1024;
+  return L;
+}
+
+// ------------------------------------------------------------------ schedule
+// Walks the contiguous range [cta*W, min(total,(cta+1)*W)) of the flattened
+// (query block, tile) space as units (query block, [t0, t1)).
+struct UnitWalk {
+  long long pos, end, W;
+  int T;
+  __device__ UnitWalk(int cta, long long W_, int G, int T_) : W(W_), T(T_) {
+    const long long total = (long long)G * T_;
+    pos = (long long)cta * W_;
+    end = pos + W_ < total ? pos + W_ : total;
+  }
+  __device__ bool next(int cta, int& qb, int& t0, int& t1, int& u_ord) {
+    if (pos >= end) return false;
+    qb = (int)(pos / T);
+    t0 = (int)(pos - (long long)qb * T);
+    const long long len = (end - pos) < (long long)(T - t0) ? (end - pos) : (long long)(T - t0);
+    t1 = t0 + (int)len;
+    u_ord = cta - (int)(((long long)qb * T) / W);
+    pos += len;
+    return true;
+  }
+};
+
+// Bounded wait that also gives up as soon as another role has aborted.
+__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (uint32_t i = 0; i < kWaitPollLimit; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 255u) == 255u) {
+      if (*abort_flag) return false;
+      if (globaltimer_ns() - t0 > kWaitTimeoutNs) return false;
+    }
+  }
+  return false;
+}
+
+__device__ __forceinline__ void raise_abort(volatile int* abort_flag, uint32_t* status, uint32_t code) {
+  *abort_flag = 1;
+  atomicOr(status, code);
+}
+
+// Filter bound on d' = ||x||^2 - 2 q.x for a pool whose k'-th key distance is
+// dstar: keys store fl(d' + ||q||^2), so admit d' <= dstar - ||q||^2 with a
+// few-ulp slack; admitting slightly more never changes the selected set, which
+// is decided by exact key order.
+__device__ __forceinline__ float bound_to_thr(float dstar, float qn) {
+  return (dstar - qn) + (fabsf(dstar) + fabsf(qn)) * 4.76837158203125e-7f;  // 2^-21
+}
+
+// ------------------------------------------------------------------ kernel
+template <int FORM>
+__global__ void __launch_bounds__(kNumThreads, 1)
+    fused_knn_kernel(const __grid_constant__ CUtensorMap tm_q_hi, const __grid_constant__ CUtensorMap tm_q_lo,
+                     const __grid_constant__ CUtensorMap tm_x_hi, const __grid_constant__ CUtensorMap tm_x_lo,
+                     const FusedParams p) {
+  using Tr = FormTraits<FORM>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const SmemLayout L = make_layout(FORM, p.d);
+  const int S = L.stages;
+
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.bar_off);
+  uint64_t* full = bars;            // [8]
+  uint64_t* empty = bars + 8;       // [8]
+  uint64_t* a_full = bars + 16;
+  uint64_t* a_empty = bars + 17;
+  uint64_t* acc_full = bars + 18;   // [2]
+  uint64_t* acc_empty = bars + 20;  // [2]
+  uint64_t* drain = bars + 22;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 23);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 24);
+  uint32_t* hist_all = reinterpret_cast<uint32_t*>(smem + L.hist_off);
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(a_full, 1);
+    mbar_init(a_empty, 1);
+    for (int s = 0; s < 2; ++s) {
+      mbar_init(&acc_full[s], 1);
+      mbar_init(&acc_empty[s], kEpiWarps);
+    }
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    fence_barrier_init();
+    fence_proxy_async_smem();
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  const int G = p.num_qblocks;
+  const int T = p.num_tiles;
+  const long long W = p.work_per_cta;
+  const int KC = Tr::kChunkElems;
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ producer
+    if (lane == 0) {
+      tma_prefetch_desc(&tm_q_hi);
+      tma_prefetch_desc(&tm_x_hi);
+      if (Tr::kAParts > 1) tma_prefetch_desc(&tm_q_lo);
+      if (Tr::kBParts > 1) tma_prefetch_desc(&tm_x_lo);
+      const uint64_t pol_db = l2_policy_evict_first();
+      const uint64_t pol_q = l2_policy_evict_last();
+      UnitWalk walk(blockIdx.x, W, G, T);
+      int qb, t0, t1, u_ord, unit = 0;
+      uint32_t it = 0;
+      bool ok = true;
+      while (ok && walk.next(blockIdx.x, qb, t0, t1, u_ord)) {
+        if (!L.a_stream) {
+          if (unit > 0 && !wait_or_abort(a_empty, (unit - 1) & 1, abort_flag)) {
+            raise_abort(abort_flag, p.status, kErrWaitTimeout);
+            ok = false;
+            break;
+          }
+          mbar_arrive_expect_tx(a_full, L.a_bytes);
+          for (int kc = 0; kc < L.nkc; ++kc)
+            for (int part = 0; part < Tr::kAParts; ++part)
+              tma_load_2d(smem + (kc * Tr::kAParts + part) * kAChunkBytes, part ? &tm_q_lo : &tm_q_hi, a_full,
+                          kc * KC, qb * kBM, pol_q);
+        }
+        for (int t = t0; t < t1 && ok; ++t) {
+          for (int kc = 0; kc < L.nkc; ++kc, ++it) {
+            const int s = (int)(it % (uint32_t)S);
+            if (!wait_or_abort(&empty[s], ((it / S) & 1u) ^ 1u, abort_flag)) {
+              raise_abort(abort_flag, p.status, kErrWaitTimeout);
+              ok = false;
+              break;
+            }
+            uint8_t* st = smem + L.a_bytes + (uint32_t)s * L.stage_bytes;
+            mbar_arrive_expect_tx(&full[s], L.stage_bytes);
+            for (int part = 0; part < Tr::kBParts; ++part)
+              tma_load_2d(st + part * kBChunkBytes, part ? &tm_x_lo : &tm_x_hi, &full[s], kc * KC, t * kBN, pol_db);
+            if (L.a_stream)
+              for (int part = 0; part < Tr::kAParts; ++part)
+                tma_load_2d(st + Tr::kBParts * kBChunkBytes + part * kAChunkBytes, part ? &tm_q_lo : &tm_q_hi,
+                            &full[s], kc * KC, qb * kBM, pol_q);
+          }
+        }
+        ++unit;
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      constexpr uint32_t fmt = Tr::kFP8 ? 0u : 1u;  // e4m3 : bf16
+      constexpr uint32_t idesc = make_idesc(fmt, fmt, kBM, kBN);
+      UnitWalk walk(blockIdx.x, W, G, T);
+      int qb, t0, t1, u_ord, unit = 0;
+      uint32_t it = 0, tc = 0;
+      bool ok = true;
+      while (ok && walk.next(blockIdx.x, qb, t0, t1, u_ord)) {
+        if (!L.a_stream) {
+          if (!wait_or_abort(a_full, unit & 1, abort_flag)) {
+            raise_abort(abort_flag, p.status, kErrWaitTimeout);
+            break;
+          }
+          tc_fence_after();
+        }
+        for (int t = t0; t < t1 && ok; ++t, ++tc) {
+          const uint32_t slot = tc & 1u, use = tc >> 1;
+          if (!wait_or_abort(&acc_empty[slot], (use & 1u) ^ 1u, abort_flag)) {
+            raise_abort(abort_flag, p.status, kErrWaitTimeout);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t d_tmem = tmem_base + slot * kBN;
+          uint32_t accumulate = 0;
+          for (int kc = 0; kc < L.nkc; ++kc, ++it) {
+            const int s = (int)(it % (uint32_t)S);
+            if (!wait_or_abort(&full[s], (it / S) & 1u, abort_flag)) {
+              raise_abort(abort_flag, p.status, kErrWaitTimeout);
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const int rem = p.d - kc * KC;
+            const int nsteps = rem >= KC ? KC / Tr::kStepElems : (rem + Tr::kStepElems - 1) / Tr::kStepElems;
+            const uint32_t st = smem_u32(smem + L.a_bytes + (uint32_t)s * L.stage_bytes);
+#pragma unroll
+            for (int pr = 0; pr < Tr::kProducts; ++pr) {
+              const uint32_t a_addr =
+                  L.a_stream ? st + Tr::kBParts * kBChunkBytes + Tr::a_part(pr) * kAChunkBytes
+                             : smem_u32(smem + (kc * Tr::kAParts + Tr::a_part(pr)) * kAChunkBytes);
+              const uint32_t b_addr = st + Tr::b_part(pr) * kBChunkBytes;
+              for (int ks = 0; ks < nsteps; ++ks) {
+                const uint64_t ad = sw128_kmajor_desc(a_addr + ks * 32);
+                const uint64_t bd = sw128_kmajor_desc(b_addr + ks * 32);
+                if (Tr::kFP8)
+                  mma_f8_ss(d_tmem, ad, bd, idesc, accumulate);
+                else
+                  mma_f16_ss(d_tmem, ad, bd, idesc, accumulate);
+                accumulate = 1;
+              }
+            }
+            mma_commit(&empty[s]);
+          }
+          if (!ok) break;
+          mma_commit(&acc_full[slot]);
+        }
+        if (!L.a_stream) mma_commit(a_empty);
+        ++unit;
+      }
+      // Make sure every issued MMA has retired before TMEM is released.
+      mma_commit(drain);
+      mbar_wait(drain, 0);
+    }
+  } else {
+    // ------------------------------------------------------------ epilogue
+    const int ew = warp - 2;       // 0..7
+    const int g = ew >> 2;         // which 128-column half of each tile
+    const int lg = warp & 3;       // TMEM lane group this warp may access
+    const int row = lg * 32 + lane;
+    uint32_t* hist = hist_all + ew * 256;
+    const uint32_t lane_base = (uint32_t)(lg * 32) << 16;
+    const int P = p.pool_cap;
+    const int U = p.units_per_block;
+    UnitWalk walk(blockIdx.x, W, G, T);
+    int qb, t0, t1, u_ord;
+    uint32_t tc = 0;
+    bool ok = true;
+    while (ok && walk.next(blockIdx.x, qb, t0, t1, u_ord)) {
+      if (u_ord < 0 || u_ord >= U) {
+        raise_abort(abort_flag, p.status, kErrBadSchedule);
+        break;
+      }
+      const int q = qb * kBM + row;
+      const bool valid = q < p.nq;
+      const float qn = valid ? p.q_norms[q] : 0.f;
+      float m2s = -2.f;
+      if (Tr::kFP8) m2s = valid ? -2.f * p.q_scale[q] : 0.f;
+      const size_t pool_row0 = (size_t)qb * kBM;  // pool index of lane-group row 0 is added per lane
+      auto pool_of = [&](int r) -> uint64_t* {
+        return p.pools + (((pool_row0 + (size_t)r) * U + (size_t)u_ord) * 2 + (size_t)g) * (size_t)P;
+      };
+      uint64_t* pool = pool_of(row);
+      int n = 0;
+      float thr = 3.402823466e38f;  // FLT_MAX: +inf norms of padding rows never pass
+
+      auto refresh = [&](uint32_t need, int keep) {
+        while (need) {
+          const int src = __ffs(need) - 1;
+          need &= need - 1;
+          const int n_src = __shfl_sync(0xffffffffu, n, src);
+          int kept = 0;
+          const uint64_t kmax =
+              warp_select_keep(pool_of(lg * 32 + src), n_src < P ? n_src : P, keep, hist, kept);
+          if (lane == src) {
+            n = kept;
+            const uint32_t ord = (uint32_t)(kmax >> 32);
+            thr = fminf(thr, bound_to_thr(ord2f(ord), qn));
+            // only a full set of k' keys bounds the global k'-th distance
+            if (kept >= p.kprime) atomicMin(&p.q_bound[q], ord);
+          }
+        }
+      };
+
+      for (int t = t0; t < t1; ++t, ++tc) {
+        const uint32_t slot = tc & 1u, use = tc >> 1;
+        if (valid) {
+          const uint32_t ob = ld_relaxed_u32(&p.q_bound[q]);
+          if (ob != kOrdInf) thr = fminf(thr, bound_to_thr(ord2f(ob), qn));
+        }
+        if (!wait_or_abort(&acc_full[slot], use & 1u, abort_flag)) {
+          raise_abort(abort_flag, p.status, kErrWaitTimeout);
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const int colh = t * kBN + g * kHalfN;
+#pragma unroll 1
+        for (int c = 0; c < kHalfN / 32; ++c) {
+          uint32_t v[32];
+          tmem_ld_32x32b_x32(tmem_base + lane_base + slot * kBN + g * kHalfN + c * 32, v);
+          tmem_ld_wait();
+          const int col0 = colh + c * 32;
+          const float4* xn4 = reinterpret_cast<const float4*>(p.db_norms + col0);
+          float dd[32];
+          bool any = false;
+#pragma unroll
+          for (int j4 = 0; j4 < 8; ++j4) {
+            const float4 xn = __ldg(xn4 + j4);
+            float a0 = __uint_as_float(v[4 * j4 + 0]), a1 = __uint_as_float(v[4 * j4 + 1]);
+            float a2 = __uint_as_float(v[4 * j4 + 2]), a3 = __uint_as_float(v[4 * j4 + 3]);
+            if (Tr::kFP8) {
+              const float4 sx = __ldg(reinterpret_cast<const float4*>(p.db_scale + col0) + j4);
+              a0 *= sx.x;
+              a1 *= sx.y;
+              a2 *= sx.z;
+              a3 *= sx.w;
+            }
+            dd[4 * j4 + 0] = fmaf(a0, m2s, xn.x);
+            dd[4 * j4 + 1] = fmaf(a1, m2s, xn.y);
+            dd[4 * j4 + 2] = fmaf(a2, m2s, xn.z);
+            dd[4 * j4 + 3] = fmaf(a3, m2s, xn.w);
+            any |= (dd[4 * j4 + 0] <= thr) | (dd[4 * j4 + 1] <= thr) | (dd[4 * j4 + 2] <= thr) |
+                   (dd[4 * j4 + 3] <= thr);
+          }
+          if (any && valid) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+              if (dd[j] <= thr) {
+                if (n < P) pool[n] = make_key(dd[j] + qn, (uint32_t)(col0 + j));
+                ++n;
+              }
+            }
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&acc_empty[slot]);
+        if (n > P) atomicOr(p.status, kErrPoolOverflow);
+        // a pool must have room for the next tile's half (kHalfN columns)
+        refresh(__ballot_sync(0xffffffffu, n > P - kHalfN), p.kprime);
+      }
+      if (!ok) break;
+      refresh(__ballot_sync(0xffffffffu, n > p.kprime), p.kprime);
+      if (valid) p.pool_counts[((pool_row0 + row) * U + u_ord) * 2 + g] = n < p.kprime ? n : p.kprime;
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem_base, 512);
+  }
+}
+
+// ------------------------------------------------------------------ host side
+namespace {
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn get_encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* ptr = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(ptr);
+  }
+  return fn;
+}
+
+// 2-D K-major operand map: rows x ld elements, box = (128 bytes of K) x box_rows,
+// 128-byte swizzle, zero fill out of bounds.
+bool make_map(CUtensorMap* m, const void* base, bool fp8, long long rows, long long ld_elems, int box_rows) {
+  EncodeTiledFn fn = get_encode_fn();
+  if (!fn) return false;
+  const int esz = fp8 ? 1 : 2;
+  cuuint64_t dims[2] = {(cuuint64_t)ld_elems, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)(ld_elems * esz)};
+  cuuint32_t box[2] = {(cuuint32_t)(kChunkBytes / esz), (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(m, fp8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
+                  const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+template <int FORM>
+cudaError_t launch_form(const FusedLaunch& f, const FusedParams& p, int grid, uint32_t smem, cudaStream_t st) {
+  static bool attr_done[16] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_done[dev & 15]) {
+    cudaError_t e = cudaFuncSetAttribute(fused_knn_kernel<FORM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         227 * 1024);
+    if (e != cudaSuccess) return e;
+    attr_done[dev & 15] = true;
+  }
+  CUtensorMap mqh, mql, mxh, mxl;
+  const bool fp8 = FORM == kFormFP8;
+  const void* qh = fp8 ? (const void*)f.q8 : (const void*)f.qh;
+  const void* xh = fp8 ? (const void*)f.x8 : (const void*)f.xh;
+  const long long ldq = fp8 ? f.ld8 : f.ld16;
+  if (!make_map(&mqh, qh, fp8, f.nq_pad, ldq, kBM) || !make_map(&mxh, xh, fp8, f.nb_pad, ldq, kBN))
+    return cudaErrorInvalidValue;
+  if (FORM == kFormExact) {
+    if (!make_map(&mql, f.ql, false, f.nq_pad, f.ld16, kBM) || !make_map(&mxl, f.xl, false, f.nb_pad, f.ld16, kBN))
+      return cudaErrorInvalidValue;
+  } else {
+    mql = mqh;
+    mxl = mxh;
+  }
+  fused_knn_kernel<FORM><<<grid, kNumThreads, smem, st>>>(mqh, mql, mxh, mxl, p);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+void plan_fused(int nq, int nb, int num_sms, FusedPlan* out) {
+  FusedPlan& pl = *out;
+  pl.num_qblocks = (nq + kBM - 1) / kBM;
+  pl.num_tiles = (nb + kBN - 1) / kBN;
+  const long long total = (long long)pl.num_qblocks * pl.num_tiles;
+  long long grid = num_sms < total ? num_sms : total;
+  if (grid < 1) grid = 1;
+  pl.work_per_cta = (total + grid - 1) / grid;
+  pl.grid = (int)((total + pl.work_per_cta - 1) / pl.work_per_cta);
+  int U = 1;
+  for (int qb = 0; qb < pl.num_qblocks; ++qb) {
+    const long long first = ((long long)qb * pl.num_tiles) / pl.work_per_cta;
+    const long long last = ((long long)(qb + 1) * pl.num_tiles - 1) / pl.work_per_cta;
+    if (last - first + 1 > U) U = (int)(last - first + 1);
+  }
+  pl.units_per_block = U;
+}
+
+uint32_t fused_smem_bytes(int form, int d) { return make_layout(form, d).total; }
+
+cudaError_t launch_fused(const FusedLaunch& f, cudaStream_t st) {
+  FusedParams p{};
+  p.nq = f.nq;
+  p.nb = f.nb;
+  p.d = f.d;
+  p.kprime = f.kprime;
+  p.pool_cap = f.pool_cap;
+  p.form = f.form;
+  p.num_qblocks = f.plan.num_qblocks;
+  p.num_tiles = f.plan.num_tiles;
+  p.work_per_cta = f.plan.work_per_cta;
+  p.units_per_block = f.plan.units_per_block;
+  p.db_norms = f.xn;
+  p.db_scale = f.xs;
+  p.q_norms = f.qn;
+  p.q_scale = f.qs;
+  p.pools = f.pools;
+  p.pool_counts = f.pool_counts;
+  p.q_bound = f.q_bound;
+  p.status = f.status;
+  const uint32_t smem = make_layout(f.form, f.d).total;
+  switch (f.form) {
+    case kFormExact:
+      return launch_form<kFormExact>(f, p, f.plan.grid, smem, st);
+    case kFormBF16:
+      return launch_form<kFormBF16>(f, p, f.plan.grid, smem, st);
+    case kFormFP8:
+      return launch_form<kFormFP8>(f, p, f.plan.grid, smem, st);
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace curplsh_b200

@@ -1,0 +1,72 @@
+// fused_knn.h -- host-side interface of the device passes (fused filter,
+// merge + rerank, row preparation).  Internal to libcurplsh_b200.so.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+
+namespace curplsh_b200 {
+
+struct FusedPlan {
+  int num_qblocks = 0;        // G = ceil(nq / 128)
+  int num_tiles = 0;          // T = ceil(nb / 256)
+  long long work_per_cta = 0; // W
+  int grid = 0;               // CTAs launched
+  int units_per_block = 0;    // U: max CTAs touching one query block
+};
+
+struct FusedLaunch {
+  int nq, nb, d, kprime, pool_cap, form;
+  long long nq_pad, nb_pad, ld16, ld8;
+  // query operands (device)
+  const __nv_bfloat16* qh;
+  const __nv_bfloat16* ql;
+  const uint8_t* q8;
+  const float* qn;
+  const float* qs;
+  // database operands (device)
+  const __nv_bfloat16* xh;
+  const __nv_bfloat16* xl;
+  const uint8_t* x8;
+  const float* xn;
+  const float* xs;
+  // outputs / scratch
+  uint64_t* pools;
+  int* pool_counts;
+  uint32_t* q_bound;
+  uint32_t* status;
+  FusedPlan plan;
+};
+
+void plan_fused(int nq, int nb, int num_sms, FusedPlan* out);
+uint32_t fused_smem_bytes(int form, int d);
+cudaError_t launch_fused(const FusedLaunch& f, cudaStream_t st);
+
+// Row preparation: squared norms (FP32), BF16 hi/lo split, FP8-E4M3 with a
+// per-row FP32 scale.  Rows in [nrows, nrows_pad) are written as zeros with
+// norm `pad_norm`.  Any of the output pointers may be null.
+cudaError_t launch_prep_rows(const float* x, long long ldx, int nrows, long long nrows_pad, int d, float* norms,
+                             float pad_norm, __nv_bfloat16* hi, __nv_bfloat16* lo, long long ld16, uint8_t* f8,
+                             float* scale, long long ld8, cudaStream_t st);
+
+// Plain squared (or not) L2 norms, as computeL2Norm.
+cudaError_t launch_l2_norms(const float* x, long long n, int d, float* norms, int squared, cudaStream_t st);
+
+struct MergeLaunch {
+  int nq, nb, d, k, kprime, pool_cap;
+  FusedPlan plan;
+  const uint64_t* pools;
+  const int* pool_counts;
+  const float* queries;   // [nq x d] fp32, row stride d
+  const float* db;        // [nb x d] fp32, row stride ld_db
+  long long ld_db;
+  int* out_idx;
+  float* out_dist;
+  uint32_t* status;
+};
+cudaError_t launch_merge_rerank(const MergeLaunch& m, cudaStream_t st);
+
+// Fill [n] ints / floats (N == 0 results, padding).
+cudaError_t launch_fill_results(int* idx, float* dist, long long n, cudaStream_t st);
+
+}  // namespace curplsh_b200

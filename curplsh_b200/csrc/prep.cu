@@ -1,0 +1,203 @@
+// prep.cu -- row preparation kernels (HBM-bound, one pass over the input).
+//
+// Replaces computeL2Norm / kernelL2Norm (cuRPLSH src/internal/norm.cu:15-202)
+// and adds the quantised operand copies the tensor-core pass reads:
+//   * squared L2 norm in FP32 (fixed reduction order: per-lane sequential over
+//     128-bit loads, then a butterfly), cached at add() time for the database;
+//   * BF16 hi = bf16(x), lo = bf16(x - hi) (the 3 x BF16 exact form);
+//   * FP8-E4M3 x / s with a per-row FP32 scale s = max|x| / 448.
+// One warp per row; 128-bit vector loads when the row allows them.  Unlike the
+// reference kernel there is no shape specialisation, so any d and any row count
+// is handled without partial-warp shuffles or out-of-bounds rows.
+#include <cuda_fp8.h>
+
+#include "common.cuh"
+#include "fused_knn.h"
+
+namespace curplsh_b200 {
+
+namespace {
+
+constexpr int kPrepWarps = 8;
+constexpr float kE4M3Max = 448.f;
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__device__ __forceinline__ uint8_t to_e4m3(float v) {
+  return (uint8_t)__nv_cvt_float_to_fp8(v, __NV_SATFINITE, __NV_E4M3);
+}
+
+__global__ void __launch_bounds__(kPrepWarps * 32) prep_rows_kernel(
+    const float* __restrict__ x, long long ldx, int nrows, long long nrows_pad, int d, float* __restrict__ norms,
+    float pad_norm, __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, long long ld16,
+    uint8_t* __restrict__ f8, float* __restrict__ scale, long long ld8, int vec4) {
+  const long long r = (long long)blockIdx.x * kPrepWarps + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (r >= nrows_pad) return;
+  if (r >= nrows) {
+    if (norms && lane == 0) norms[r] = pad_norm;
+    if (scale && lane == 0) scale[r] = 0.f;
+    if (hi)
+      for (long long i = lane; i < ld16; i += 32) hi[r * ld16 + i] = __float2bfloat16_rn(0.f);
+    if (lo)
+      for (long long i = lane; i < ld16; i += 32) lo[r * ld16 + i] = __float2bfloat16_rn(0.f);
+    if (f8)
+      for (long long i = lane; i < ld8; i += 32) f8[r * ld8 + i] = 0;
+    return;
+  }
+  const float* row = x + r * ldx;
+  float s = 0.f, m = 0.f;
+  if (vec4) {
+    const float4* row4 = reinterpret_cast<const float4*>(row);
+    for (int i = lane; i < d / 4; i += 32) {
+      const float4 v = __ldg(row4 + i);
+      s = fmaf(v.x, v.x, s);
+      s = fmaf(v.y, v.y, s);
+      s = fmaf(v.z, v.z, s);
+      s = fmaf(v.w, v.w, s);
+      m = fmaxf(m, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
+    }
+  } else {
+    for (int i = lane; i < d; i += 32) {
+      const float v = __ldg(row + i);
+      s = fmaf(v, v, s);
+      m = fmaxf(m, fabsf(v));
+    }
+  }
+  s = warp_sum(s);
+  if (norms && lane == 0) norms[r] = s;
+  if (!hi && !lo && !f8) return;
+  float inv = 1.f;
+  if (f8) {
+    m = warp_max(m);
+    const float sc = m > 0.f ? m / kE4M3Max : 1.f;
+    inv = 1.f / sc;
+    if (scale && lane == 0) scale[r] = sc;
+  }
+  if (vec4) {
+    const float4* row4 = reinterpret_cast<const float4*>(row);
+    for (int i = lane; i < d / 4; i += 32) {
+      const float4 v = __ldg(row4 + i);
+      if (hi) {
+        const __nv_bfloat16 h0 = __float2bfloat16_rn(v.x), h1 = __float2bfloat16_rn(v.y);
+        const __nv_bfloat16 h2 = __float2bfloat16_rn(v.z), h3 = __float2bfloat16_rn(v.w);
+        __nv_bfloat162 a, b;
+        a.x = h0; a.y = h1; b.x = h2; b.y = h3;
+        uint2 pk;
+        pk.x = *reinterpret_cast<uint32_t*>(&a);
+        pk.y = *reinterpret_cast<uint32_t*>(&b);
+        *reinterpret_cast<uint2*>(hi + r * ld16 + 4 * i) = pk;
+        if (lo) {
+          __nv_bfloat162 c, e;
+          c.x = __float2bfloat16_rn(v.x - __bfloat162float(h0));
+          c.y = __float2bfloat16_rn(v.y - __bfloat162float(h1));
+          e.x = __float2bfloat16_rn(v.z - __bfloat162float(h2));
+          e.y = __float2bfloat16_rn(v.w - __bfloat162float(h3));
+          uint2 pl;
+          pl.x = *reinterpret_cast<uint32_t*>(&c);
+          pl.y = *reinterpret_cast<uint32_t*>(&e);
+          *reinterpret_cast<uint2*>(lo + r * ld16 + 4 * i) = pl;
+        }
+      }
+      if (f8) {
+        const uint32_t q = (uint32_t)to_e4m3(v.x * inv) | ((uint32_t)to_e4m3(v.y * inv) << 8) |
+                           ((uint32_t)to_e4m3(v.z * inv) << 16) | ((uint32_t)to_e4m3(v.w * inv) << 24);
+        *reinterpret_cast<uint32_t*>(f8 + r * ld8 + 4 * i) = q;
+      }
+    }
+    if (hi)
+      for (long long i = d + lane; i < ld16; i += 32) {
+        hi[r * ld16 + i] = __float2bfloat16_rn(0.f);
+        if (lo) lo[r * ld16 + i] = __float2bfloat16_rn(0.f);
+      }
+    if (f8)
+      for (long long i = d + lane; i < ld8; i += 32) f8[r * ld8 + i] = 0;
+  } else {
+    if (hi)
+      for (long long i = lane; i < ld16; i += 32) {
+        const float v = i < d ? row[i] : 0.f;
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        hi[r * ld16 + i] = h;
+        if (lo) lo[r * ld16 + i] = __float2bfloat16_rn(v - __bfloat162float(h));
+      }
+    if (f8)
+      for (long long i = lane; i < ld8; i += 32) {
+        const float v = i < d ? row[i] : 0.f;
+        f8[r * ld8 + i] = to_e4m3(v * inv);
+      }
+  }
+}
+
+__global__ void __launch_bounds__(kPrepWarps * 32)
+    l2_norms_kernel(const float* __restrict__ x, long long n, int d, float* __restrict__ norms, int squared,
+                    int vec4) {
+  const long long r = (long long)blockIdx.x * kPrepWarps + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (r >= n) return;
+  const float* row = x + r * (long long)d;
+  float s = 0.f;
+  if (vec4) {
+    const float4* row4 = reinterpret_cast<const float4*>(row);
+    for (int i = lane; i < d / 4; i += 32) {
+      const float4 v = __ldg(row4 + i);
+      s = fmaf(v.x, v.x, s);
+      s = fmaf(v.y, v.y, s);
+      s = fmaf(v.z, v.z, s);
+      s = fmaf(v.w, v.w, s);
+    }
+  } else {
+    for (int i = lane; i < d; i += 32) {
+      const float v = __ldg(row + i);
+      s = fmaf(v, v, s);
+    }
+  }
+  s = warp_sum(s);
+  if (lane == 0) norms[r] = squared ? s : sqrtf(s);
+}
+
+__global__ void fill_results_kernel(int* idx, float* dist, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    if (idx) idx[i] = -1;
+    if (dist) dist[i] = 3.402823466e38f;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_prep_rows(const float* x, long long ldx, int nrows, long long nrows_pad, int d, float* norms,
+                             float pad_norm, __nv_bfloat16* hi, __nv_bfloat16* lo, long long ld16, uint8_t* f8,
+                             float* scale, long long ld8, cudaStream_t st) {
+  if (nrows_pad <= 0) return cudaSuccess;
+  const int vec4 = (d % 4 == 0) && (ldx % 4 == 0) && ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
+  const long long blocks = (nrows_pad + kPrepWarps - 1) / kPrepWarps;
+  prep_rows_kernel<<<(unsigned)blocks, kPrepWarps * 32, 0, st>>>(x, ldx, nrows, nrows_pad, d, norms, pad_norm, hi,
+                                                                 lo, ld16, f8, scale, ld8, vec4);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_l2_norms(const float* x, long long n, int d, float* norms, int squared, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const int vec4 = (d % 4 == 0) && ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
+  const long long blocks = (n + kPrepWarps - 1) / kPrepWarps;
+  l2_norms_kernel<<<(unsigned)blocks, kPrepWarps * 32, 0, st>>>(x, n, d, norms, squared, vec4);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill_results(int* idx, float* dist, long long n, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  long long blocks = (n + 255) / 256;
+  if (blocks > 4096) blocks = 4096;
+  fill_results_kernel<<<(unsigned)blocks, 256, 0, st>>>(idx, dist, n);
+  return cudaGetLastError();
+}
+
+}  // namespace curplsh_b200

@@ -1,0 +1,151 @@
+/*
+ * curplsh_b200.h -- C ABI of the B200-native exact L2 kNN engine.
+ *
+ * Plain pointers and sizes only (no C++ or framework types), status-code
+ * errors.  Every entry point says which cuRPLSH interface it replaces
+ * (paths are relative to the cuRPLSH source tree).  The C++ drop-in headers
+ * under include/curplsh/ (Index, IndexBF, DeviceResources, tensors) are thin
+ * inline wrappers over these functions, and the Python package
+ * curplsh_b200 binds them with ctypes.
+ *
+ * Pointer arguments named "data", "queries", "indices", "distances" may be
+ * host or device memory (detected with cudaPointerGetAttributes), as in the
+ * reference (include/device_tensor.h:173-185, src/index_bf.cpp:56-73).
+ *
+ * Errors: every function returns CURPLSH_OK (0) or a CURPLSH_ERR_* code and
+ * records a message for curplsh_last_error() (thread-local).  The reference
+ * aborts or exits instead (include/internal/assertions.h:7-14,
+ * include/internal/cuda_utils.h:991-1001).
+ */
+#ifndef CURPLSH_B200_H_
+#define CURPLSH_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+#define CURPLSH_OK 0
+#define CURPLSH_ERR_INVALID_ARG 1 /* bad argument (null, k out of range, dim mismatch) */
+#define CURPLSH_ERR_CUDA 2        /* a CUDA runtime call failed */
+#define CURPLSH_ERR_OOM 3         /* device or host allocation failed */
+#define CURPLSH_ERR_UNSUPPORTED 4 /* valid request this build does not implement */
+#define CURPLSH_ERR_DEVICE 5      /* a kernel reported an internal failure (bounded wait expired, overflow) */
+#define CURPLSH_ERR_STATE 6       /* call not valid in the object's current state */
+
+/* ------------------------------------------------------------ enums */
+/* MemorySpace (include/memory_space.h:12-17) */
+#define CURPLSH_MEMORY_DEVICE 0
+#define CURPLSH_MEMORY_UNIFIED 1
+
+/* Precision form of the coarse tensor-core pass; every form ends with an exact
+ * FP32 rerank, so returned distances are FP32 squared L2 in all forms. */
+#define CURPLSH_PRECISION_FP32_EXACT 0  /* 3 x BF16 split products, k' = k + margin */
+#define CURPLSH_PRECISION_BF16_RERANK 1 /* BF16 coarse, k' = rerank_factor * k */
+#define CURPLSH_PRECISION_FP8_RERANK 2  /* FP8-E4M3 (per-vector FP32 scale), k' = rerank_factor * k */
+
+/* ------------------------------------------------------------ opaque handles */
+typedef struct curplsh_resources curplsh_resources; /* DeviceResources (include/device_resources.h:60-263) */
+typedef struct curplsh_index curplsh_index;         /* Index / IndexBF (include/index.h:18-82, include/index_bf.h:21-46) */
+
+/* IndexBFConfig (include/index_bf.h:8-19) including its IndexConfig base
+ * (include/index.h:8-16), plus the engine's precision controls. */
+typedef struct curplsh_bf_config {
+  int32_t device;                  /* IndexConfig::device */
+  int32_t memory_space;            /* IndexConfig::memorySpace (CURPLSH_MEMORY_*) */
+  int32_t store_transposed;        /* IndexBFConfig::storeTransposed: accepted, layout is always the
+                                      engine's K-major tiled copy (the reference leaves it a TODO) */
+  int32_t compute_exact_distances; /* IndexBFConfig::computeExactDistances: IndexBF::search always
+                                      returns exact squared distances (src/index_bf.cpp:68-69), so is this */
+  int32_t precision;               /* CURPLSH_PRECISION_* default for search */
+  int32_t rerank_factor;           /* k' = rerank_factor * k for the BF16/FP8 forms (default 4) */
+  int32_t borrow_device_data;      /* 1: add() of device memory keeps a reference to the caller's FP32
+                                      rows (the reference's aliasing, include/device_tensor.h:97-103);
+                                      0 (default): the index copies them */
+} curplsh_bf_config;
+
+/* Defaults: device 0, device memory, FP32-exact, rerank_factor 4, copy on add. */
+void curplsh_bf_config_init(curplsh_bf_config* cfg);
+
+const char* curplsh_last_error(void);
+const char* curplsh_version(void);
+
+/* getNumDevices (include/internal/cuda_utils.h:1230-1258) */
+int curplsh_get_num_devices(int* out);
+
+/* ------------------------------------------------------------ DeviceResources */
+/* DeviceResources() (include/device_resources.h:62) */
+int curplsh_resources_create(curplsh_resources** out);
+/* ~DeviceResources (include/device_resources.h:72-108) */
+int curplsh_resources_destroy(curplsh_resources* res);
+/* initializeForDevice (include/device_resources.h:113-165) */
+int curplsh_resources_initialize_for_device(curplsh_resources* res, int device);
+/* getDefaultStream (include/device_resources.h:181-184) */
+int curplsh_resources_get_default_stream(curplsh_resources* res, int device, void** stream);
+/* user default stream (include/device_resources.h:247-248, a map the reference never fills);
+ * must be called before the device is initialised */
+int curplsh_resources_set_default_stream(curplsh_resources* res, int device, void* stream);
+/* getAlternateStreams (include/device_resources.h:187-190); writes up to *count streams */
+int curplsh_resources_get_alternate_streams(curplsh_resources* res, int device, void** streams, int* count);
+/* getAsyncCopyStream (include/device_resources.h:199-201) */
+int curplsh_resources_get_async_copy_stream(curplsh_resources* res, int device, void** stream);
+/* syncDefaultStream (include/device_resources.h:220-222) */
+int curplsh_resources_sync_default_stream(curplsh_resources* res, int device);
+
+/* ------------------------------------------------------------ Index / IndexBF */
+/* IndexBF(DeviceResources*, int dim, IndexBFConfig) (include/index_bf.h:23-24, src/index.cpp:8-27) */
+int curplsh_index_bf_create(curplsh_resources* res, int dim, const curplsh_bf_config* cfg,
+                            curplsh_index** out);
+/* ~IndexBF */
+int curplsh_index_destroy(curplsh_index* index);
+/* Index::train (include/index.h:29); brute force needs none: a no-op, as src/index_bf.cpp:13-15 */
+int curplsh_index_train(curplsh_index* index, int64_t num, const float* data);
+/* Index::add (include/index.h:38, src/index_bf.cpp:26-44): rows get sequential labels; squared norms and
+ * the quantised operand copies are computed once here.  Unlike the reference (one add only,
+ * index_bf.cpp:27) further adds append. */
+int curplsh_index_add(curplsh_index* index, int64_t num, const float* data);
+/* Index::search (include/index.h:52-53, src/index_bf.cpp:46-74): k nearest rows of every query,
+ * ascending squared L2 distance, ties by lower row index; slots beyond the number of rows are
+ * (-1, FLT_MAX).  k must be in [1, 1024] (search.cu:121-122).  Uses the index's default precision,
+ * runs on the resources' default stream and returns when the results are in place. */
+int curplsh_index_search(curplsh_index* index, int64_t num, const float* queries, int k, int* indices,
+                         float* distances);
+/* search with an explicit precision form (-1: index default), rerank factor (<= 0: index default)
+ * and stream (NULL: default stream).  When queries, indices and distances are all device memory the
+ * call is asynchronous on `stream`; otherwise it synchronises before returning. */
+int curplsh_index_search_ex(curplsh_index* index, int64_t num, const float* queries, int k, int precision,
+                            int rerank_factor, int* indices, float* distances, void* stream);
+/* As curplsh_index_search_ex, synchronous, also returning device-timed milliseconds of the passes
+ * (CUDA events on the launching stream): pass_ms[0] query prep, [1] fused tensor-core filter,
+ * [2] merge + exact rerank, [3] whole search including any host<->device copies. */
+int curplsh_index_search_profiled(curplsh_index* index, int64_t num, const float* queries, int k,
+                                  int precision, int rerank_factor, int* indices, float* distances,
+                                  void* stream, float* pass_ms);
+/* Index::reset (include/index.h:56, src/index_bf.cpp:17-24) */
+int curplsh_index_reset(curplsh_index* index);
+/* getDimension / getNumData / getDevice (include/index.h:58-64) */
+int curplsh_index_get_dimension(const curplsh_index* index, int* out);
+int curplsh_index_get_num_data(const curplsh_index* index, int64_t* out);
+int curplsh_index_get_device(const curplsh_index* index, int* out);
+
+/* ------------------------------------------------------------ free functions */
+/* computeL2Norm (include/internal/norm.h:7-8, src/internal/norm.cu:191-202): device pointers,
+ * vectors [num x dim] row-major, norms [num]; squared != 0 gives squared norms. */
+int curplsh_compute_l2_norm(const float* vectors, int64_t num, int dim, float* norms, int squared,
+                            void* stream);
+/* searchL2Distance (include/internal/search.h:7-11, src/internal/search.cu:79-216) over device
+ * buffers: bases [nb x dim], queries [nq x dim], indices/distances [nq x k].  base_norms is accepted
+ * for signature parity and may be NULL (norms are recomputed in the engine's own layout).
+ * exact_distances != 0 returns ||q - x||^2; 0 returns the reference's relative form
+ * ||x||^2 - 2 q.x (= exact - ||q||^2).  Synchronous. */
+int curplsh_search_l2_distance(curplsh_resources* res, const float* bases, int64_t nb, const float* base_norms,
+                               const float* queries, int64_t nq, int dim, int k, int* indices,
+                               float* distances, int exact_distances);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* CURPLSH_B200_H_ */

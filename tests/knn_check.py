@@ -1,0 +1,57 @@
+"""Shared parity assertions for the GPU tests (CUDA result vs the FP64 oracle)."""
+import numpy as np
+
+import oracle
+
+FLT_MAX = np.float32(np.finfo(np.float32).max)
+
+# Distances: the engine returns sum (q-x)^2 evaluated in FP32 after an exact
+# rerank; the tolerance is relative 1e-4 (plus a tiny absolute floor for
+# distances at or near zero).
+DIST_RTOL = 1e-4
+DIST_ATOL_FRAC = 1e-6   # of the mean squared norm scale
+# Indices: strict positional equality wherever the oracle's neighbouring
+# distances are separated by more than this (relative); tie-aware recall 1.0
+# everywhere.
+SEP_RTOL = 1e-5
+
+
+def assert_knn_matches(base, queries, got_d, got_i, ref_d, ref_i, min_recall=1.0, strict=True):
+    base = np.asarray(base, np.float32)
+    queries = np.asarray(queries, np.float32)
+    got_d = np.asarray(got_d, np.float64)
+    got_i = np.asarray(got_i, np.int64)
+    nq, k = got_i.shape
+    ref_d = ref_d[:, :k + 1] if ref_d.shape[1] > k else ref_d
+    ref_i = ref_i[:, :k]
+    rk = ref_d[:, :k]
+    scale = float(np.mean(np.sum(base.astype(np.float64) ** 2, 1))) if base.size else 1.0
+    atol = DIST_ATOL_FRAC * max(scale, 1e-30)
+    pad = ref_i < 0
+    assert np.array_equal(got_i < 0, pad), "padding slots differ"
+    assert (got_d[pad] == FLT_MAX).all(), "padding distances must be FLT_MAX"
+    real = ~pad
+    # distances at each rank
+    err = np.abs(got_d[real] - rk[real])
+    lim = DIST_RTOL * np.abs(rk[real]) + atol
+    assert (err <= lim).all(), f"distance error max {err.max():.3e} (limit {lim[np.argmax(err - lim)]:.3e})"
+    # returned distance belongs to the returned index
+    qidx = np.repeat(np.arange(nq), k).reshape(nq, k)
+    own = oracle.exact_distances(base, queries, qidx, got_i)
+    e2 = np.abs(got_d[real] - own[real])
+    assert (e2 <= DIST_RTOL * np.abs(own[real]) + atol).all(), "returned distance does not match its index"
+    # ascending order
+    gd = np.where(real, got_d, np.inf)
+    assert (np.diff(gd, axis=1) >= 0).all(), "results not sorted"
+    # recall (tie-aware)
+    rec, per = oracle.recall_at_k(base, queries, got_i, rk)
+    assert rec >= min_recall, f"recall {rec:.6f} < {min_recall} (worst query {per.min():.3f})"
+    if strict and min_recall >= 1.0:
+        full = np.concatenate([ref_d, np.full((nq, max(0, k + 1 - ref_d.shape[1])), np.inf)], axis=1)[:, :k + 1]
+        lo = np.concatenate([np.full((nq, 1), -np.inf), full[:, :k - 1]], axis=1)
+        sep = ((full[:, :k] - lo) > SEP_RTOL * np.abs(full[:, :k])) & \
+              ((full[:, 1:k + 1] - full[:, :k]) > SEP_RTOL * np.abs(full[:, :k]))
+        sep &= real
+        bad = sep & (got_i != ref_i)
+        assert not bad.any(), f"{int(bad.sum())} well-separated positions differ, first at {np.argwhere(bad)[0]}"
+    return rec
