@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
 #include <cstdarg>
 #include <cstdio>
@@ -150,10 +151,14 @@ struct DevRes {
   int num_sms = 0;
 };
 
+// Reference counted: every index holds a reference, so destroying the
+// resources while indexes are alive only drops the caller's reference and the
+// streams live until the last index is destroyed.
 struct curplsh_resources {
   std::mutex mu;
   std::map<int, DevRes> devs;
   std::map<int, cudaStream_t> user_default;
+  std::atomic<int> refs{1};
 };
 
 namespace {
@@ -252,6 +257,12 @@ int kprime_for(int form, int k, int rerank_factor, int64_t n) {
   return (int)kp;
 }
 
+// Pool capacity: k' kept keys + room for one half tile + refresh headroom.  A
+// refresh (warp radix select, cost ~ capacity) runs only when fewer than one
+// half tile of free slots remain, so each refresh absorbs >= max(k', 256)
+// survivors and refreshes stay rare.
+int pool_capacity(int kp) { return (int)round_up(kp + kHalfN + std::max(kp, 256), 32); }
+
 struct Timing {
   cudaEvent_t ev[5] = {};
   bool on = false;
@@ -282,7 +293,7 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
     if (rc) return rc;
   }
   const int kp = kprime_for(form, k, rerank_factor, ix->n);
-  const int P = (int)round_up(kp + kHalfN, 32);
+  const int P = pool_capacity(kp);
   FusedPlan plan;
   plan_fused(nq, (int)ix->n, ix->dres->num_sms, &plan);
   const long long nq_pad = round_up(nq, kBM);
@@ -356,7 +367,7 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
 size_t search_workspace_bytes(const curplsh_index* ix, int nq, int k, int form, int rerank_factor) {
   if (ix->n == 0) return 0;
   const int kp = kprime_for(form, k, rerank_factor, ix->n);
-  const int P = (int)round_up(kp + kHalfN, 32);
+  const int P = pool_capacity(kp);
   FusedPlan plan;
   plan_fused(nq, (int)ix->n, ix->dres->num_sms, &plan);
   const long long nq_pad = round_up(nq, kBM);
@@ -497,8 +508,8 @@ int curplsh_resources_create(curplsh_resources** out) {
   return *out ? CURPLSH_OK : set_error(CURPLSH_ERR_OOM, "host allocation");
 }
 
-int curplsh_resources_destroy(curplsh_resources* r) {
-  if (!r) return CURPLSH_OK;
+static void resources_release(curplsh_resources* r) {
+  if (r->refs.fetch_sub(1) != 1) return;
   for (auto& kv : r->devs) {
     DeviceScope scope(kv.first);
     DevRes& d = kv.second;
@@ -508,6 +519,11 @@ int curplsh_resources_destroy(curplsh_resources* r) {
     cudaStreamDestroy(d.copy);
   }
   delete r;
+}
+
+int curplsh_resources_destroy(curplsh_resources* r) {
+  if (!r) return CURPLSH_OK;
+  resources_release(r);
   return CURPLSH_OK;
 }
 
@@ -591,12 +607,14 @@ int curplsh_index_bf_create(curplsh_resources* r, int dim, const curplsh_bf_conf
   ix->dres = d;
   ix->ld16 = round_up(dim, 8);
   ix->ld8 = round_up(dim, 16);
+  r->refs.fetch_add(1);
   DeviceScope scope(c.device);
   cudaError_t e = cudaMalloc(&ix->status, sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaMemset(ix->status, 0, sizeof(uint32_t));
   if (e != cudaSuccess) {
     cudaGetLastError();
     delete ix;
+    resources_release(r);
     return set_error(CURPLSH_ERR_CUDA, "status word: %s", cudaGetErrorString(e));
   }
   *out = ix;
@@ -616,7 +634,9 @@ int curplsh_index_destroy(curplsh_index* ix) {
     ix->free_db();
     if (ix->status) cudaFree(ix->status);
   }
+  curplsh_resources* r = ix->res;
   delete ix;
+  resources_release(r);
   return CURPLSH_OK;
 }
 
