@@ -1,0 +1,345 @@
+"""Benchmark: exact L2 kNN search throughput on one B200 (or N replicas).
+
+Workload (one "step" = one IndexBF search of the whole query batch): the
+Gaussian-mixture configuration -- N = 1,000,000 database rows, Q = 10,000
+queries, d = 128, k = 100, integer-valued FP32 data from 1,000 centroids
+(seeded synthetic data, see curplsh_b200/synth.py).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints ONE JSON line (rank 0).  `value` is queries/s of the headline form
+(BF16 coarse + exact FP32 rerank) with queries resident in HBM, kernels timed
+with CUDA events on the launching stream; `e2e` is the same metric through the
+C ABI with pinned host buffers (H2D of the queries and D2H of the results inside
+the timed region).  Every form's recall@k is checked against the FP64 oracle on
+a query subsample; `cpu_baseline` times that oracle on the host cores.
+
+Multi-GPU (torchrun): each rank searches its own query batch against a
+replicated database (weak scaling, no collective on the data path); timing is
+the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "mixture_int_1m"
+N_DB, N_Q, DIM, K = 1_000_000, 10_000, 128, 100
+FORMS = {0: "fp32_exact", 1: "bf16_rerank", 2: "fp8_rerank"}
+HEADLINE_FORM = 1
+RECALL_SAMPLE = 128       # queries checked against the oracle per form
+METRIC = "queries/s at recall@k=1.0"
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), d.get("bf16_tflops_sustained"), "measured"
+    return 6650.0, 1590.0, 1400.0, "fallback"
+
+
+def load_traffic(form_name):
+    """DRAM bytes per fused launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "fused_knn_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    return d.get(WORKLOAD, {}).get(form_name)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        cmd = ["nvidia-smi", "-i", str(self.index),
+               "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+               "--format=csv,noheader,nounits", "-lms", "50"]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        time.sleep(0.25)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_oracle_rate(base_h, q_h, k, nq_sample):
+    import oracle
+    t0 = time.perf_counter()
+    dist_, idx_ = oracle.knn(base_h, q_h[:nq_sample], k + 1)
+    dt = time.perf_counter() - t0
+    return nq_sample / dt, dist_, idx_, oracle.num_threads()
+
+
+def run_reference(args, world, rank):
+    """--impl reference: the reference has no CPU path of its own; its search
+    semantics (search.cu:79-216) are restated by the FP64 host oracle, timed
+    here on all host cores over a bounded query sample per step."""
+    if rank != 0:
+        return 0
+    import numpy as np
+    import torch
+
+    import oracle
+    from curplsh_b200 import synth
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    base, queries, k = synth.make(WORKLOAD, device=dev)
+    base_h = base.cpu().numpy()
+    q_h = queries.cpu().numpy()
+    sample = 128
+    for w in range(args.warmup):
+        oracle.knn(base_h, q_h[w * sample:(w + 1) * sample], k)
+    times = []
+    for s in range(args.steps):
+        off = ((args.warmup + s) * sample) % (q_h.shape[0] - sample)
+        t0 = time.perf_counter()
+        oracle.knn(base_h, q_h[off:off + sample], k)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    qps = sample * args.steps / total
+    cores = oracle.num_threads()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian mixture, integer-valued)",
+        "config": {"workload": WORKLOAD, "N": N_DB, "Q": N_Q, "d": DIM, "k": K, "q_per_step_sample": sample},
+        "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": cores, "kind": "port",
+                         "sample": f"{sample} queries per step against all {N_DB} rows"},
+        "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference ships no CPU search; this arm times the FP64 restatement of its searchL2Distance "
+                "semantics (oracle/knn_oracle.c) on the host cores",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local = dist_init()
+    if args.impl == "reference":
+        rc = run_reference(args, world, rank)
+        barrier(world)
+        return rc
+
+    import numpy as np
+    import torch
+
+    import curplsh_b200 as cb
+    import oracle
+    from curplsh_b200 import synth
+
+    torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
+    # every rank holds the same database and searches a full query batch (replicas)
+    base, queries, k = synth.make(WORKLOAD, device=dev)
+    res = cb.DeviceResources(local)
+    stream = torch.cuda.Stream(device=dev)
+    Q = queries.shape[0]
+    oi = torch.empty((Q, k), dtype=torch.int32, device=dev)
+    od = torch.empty((Q, k), dtype=torch.float32, device=dev)
+
+    # ---- recall of every form on a query subsample (rank 0), and the CPU baseline
+    sub = torch.arange(0, Q, Q // RECALL_SAMPLE, device=dev)[:RECALL_SAMPLE]
+    form_results = {}
+    cpu = None
+    if rank == 0:
+        base_h = base.cpu().numpy()
+        qs_h = queries[sub].cpu().numpy()
+        rate, rd, ri, cores = cpu_oracle_rate(base_h, qs_h, k, RECALL_SAMPLE)
+        cpu = {"value": rate, "unit": "queries/s", "cores": cores, "kind": "port",
+               "sample": f"{RECALL_SAMPLE} queries against all {N_DB} rows (FP64 oracle, OpenMP)"}
+    indexes = {}
+    for form in FORMS:
+        ix = cb.IndexBF(res, DIM, cb.IndexBFConfig(device=local, precision=form))
+        ix.add(N_DB, base)
+        indexes[form] = ix
+        ix.search_ex(Q, queries, k, oi, od, stream=stream)
+        stream.synchronize()
+        if rank == 0:
+            gi = oi[sub].cpu().numpy()
+            gd = od[sub].cpu().numpy().astype(np.float64)
+            rec, _ = oracle.recall_at_k(base_h, qs_h, gi, rd[:, :k])
+            err = float(np.max(np.abs(gd - rd[:, :k]) / np.maximum(np.abs(rd[:, :k]), 1e-30)))
+            form_results[FORMS[form]] = {"recall_at_k": rec, "max_rel_dist_err": err}
+
+    # ---- timed region: device-resident queries, CUDA events on our stream
+    peaks = load_peaks()
+    flops = 2.0 * Q * N_DB * DIM
+    launches_per_step = 3  # query prep, fused tensor-core filter, merge + rerank
+    timing = {}
+    clocks = None
+    for form in FORMS:
+        ix = indexes[form]
+        for _ in range(args.warmup):
+            ix.search_ex(Q, queries, k, oi, od, stream=stream)
+        stream.synchronize()
+        barrier(world)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        sampler = ClockSampler(local) if form == HEADLINE_FORM else None
+        if sampler:
+            sampler.__enter__()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            ix.search_ex(Q, queries, k, oi, od, stream=stream)
+        ev1.record(stream)
+        ev1.synchronize()
+        if sampler:
+            sampler.__exit__(None, None, None)
+            clocks = sampler.summary()
+        ms = ev0.elapsed_time(ev1) / args.steps
+        ms = max_over_ranks(ms, world)
+        # per-pass device times (events between passes on the same stream)
+        passes = ix.search_profiled(Q, queries, k, oi, od, stream=stream)
+        fused_ms = max_over_ranks(passes["fused_ms"], world)
+        timing[form] = (ms, fused_ms, passes)
+
+    # ---- end to end through the C ABI: pinned host queries in, host results out
+    qh = torch.empty((Q, DIM), dtype=torch.float32, pin_memory=True)
+    qh.copy_(queries.cpu())
+    ih = torch.empty((Q, k), dtype=torch.int32, pin_memory=True)
+    dh = torch.empty((Q, k), dtype=torch.float32, pin_memory=True)
+    ix = indexes[HEADLINE_FORM]
+    for _ in range(args.warmup):
+        ix.search(Q, qh, k, ih, dh)
+    barrier(world)
+    e2e_ms = []
+    for _ in range(args.steps):
+        t = ix.search_profiled(Q, qh, k, ih, dh, stream=stream)
+        e2e_ms.append(t["total_ms"])
+    e2e = max_over_ranks(sum(e2e_ms) / len(e2e_ms), world)
+
+    if rank == 0:
+        ms, fused_ms, passes = timing[HEADLINE_FORM]
+        hbm, bf16_burst, bf16_sust, peak_kind = peaks
+        forms_out = {}
+        for form, name in FORMS.items():
+            f_ms, f_fused, _ = timing[form]
+            p_form = bf16_burst / 3.0 if form == 0 else (2 * bf16_burst if form == 2 else bf16_burst)
+            forms_out[name] = {
+                "queries_per_s": Q * world / (f_ms / 1e3), "ms_per_search": f_ms, "fused_ms": f_fused,
+                "fused_tflops": flops / (f_fused / 1e3) / 1e12,
+                "roofline_frac": flops / (f_fused / 1e3) / 1e12 / p_form,
+                "peak_basis_tflops": p_form, **form_results.get(name, {}),
+            }
+        achieved = flops / (fused_ms / 1e3) / 1e12
+        rec_ok = form_results[FORMS[HEADLINE_FORM]]["recall_at_k"] >= 1.0
+        line = {
+            "metric": METRIC, "value": Q * world / (ms / 1e3), "unit": "queries/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
+            "data": "synthetic (seeded Gaussian mixture, 1000 centroids, sigma 12, integer-valued FP32)",
+            "config": {"workload": WORKLOAD, "N": N_DB, "Q": Q, "d": DIM, "k": k, "form": FORMS[HEADLINE_FORM],
+                       "rerank_factor": 4, "l2": "database (1.0 GB FP32 + 0.5 GB BF16 copies) larger than L2",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "recall_at_k": form_results[FORMS[HEADLINE_FORM]]["recall_at_k"], "recall_ok": rec_ok,
+            "forms": forms_out,
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": bf16_burst, "unit": "TFLOP/s",
+                         "frac": achieved / bf16_burst, "traffic": load_traffic(FORMS[HEADLINE_FORM]),
+                         "kernel": "fused_knn_kernel<BF16>", "peak_kind": peak_kind + " bf16 burst",
+                         "algorithmic": "2*Q*N*d flops per launch"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": Q * world / (e2e / 1e3), "unit": "queries/s", "ms_per_step": e2e,
+                    "h2d_bytes_per_step": Q * DIM * 4, "d2h_bytes_per_step": Q * k * 8},
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clocks,
+            "passes_ms": {k_: v for k_, v in passes.items()},
+        }
+        print(json.dumps(line), flush=True)
+    for ix in indexes.values():
+        ix.close()
+    res.close()
+    barrier(world)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -26,7 +26,8 @@ __all__ = [
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB_PATH = os.path.join(_HERE, "libcurplsh_b200.so")
+# CURPLSH_B200_LIB selects another build of the library (e.g. an instrumented one).
+_LIB_PATH = os.environ.get("CURPLSH_B200_LIB") or os.path.join(_HERE, "libcurplsh_b200.so")
 
 
 class CurplshError(RuntimeError):

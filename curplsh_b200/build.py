@@ -20,6 +20,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libcurplsh_b200.so")
+EXTRA_DEFINES: list[str] = []  # e.g. ["-DCURPLSH_FUSED_STATS"] for an instrumented build
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
@@ -43,12 +44,13 @@ def headers():
 
 def _compile(src: str, force: bool, verbose_ptxas: bool) -> str:
     obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+    common = COMMON + EXTRA_DEFINES
     newest_dep = max(os.path.getmtime(p) for p in headers() + [src])
     if not force and os.path.exists(obj) and os.path.getmtime(obj) >= newest_dep:
         return obj
-    cmd = [nvcc(), *ARCH, *COMMON, "-c", src, "-o", obj]
+    cmd = [nvcc(), *ARCH, *common, "-c", src, "-o", obj]
     if src.endswith(".cpp"):
-        cmd = [nvcc(), *COMMON, "-x", "cu", *ARCH, "-c", src, "-o", obj]
+        cmd = [nvcc(), *common, "-x", "cu", *ARCH, "-c", src, "-o", obj]
     if verbose_ptxas and src.endswith(".cu"):
         cmd.insert(1, "-Xptxas=-v")
     res = subprocess.run(cmd, capture_output=True, text=True)
@@ -59,7 +61,15 @@ def _compile(src: str, force: bool, verbose_ptxas: bool) -> str:
     return obj
 
 
-def build(force: bool = False, verbose_ptxas: bool = False) -> str:
+def build(force: bool = False, verbose_ptxas: bool = False, build_dir: str | None = None,
+          lib: str | None = None) -> str:
+    """Compile every source under csrc/ and link the shared library.  build_dir
+    and lib redirect the outputs (used for instrumented side builds)."""
+    global BUILD, LIB
+    if build_dir:
+        BUILD = build_dir
+    if lib:
+        LIB = lib
     os.makedirs(BUILD, exist_ok=True)
     srcs = sources()
     with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:

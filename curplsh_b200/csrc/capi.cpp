@@ -341,7 +341,29 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
   f.q_bound = qbound;
   f.status = ix->status;
   f.plan = plan;
+#ifdef CURPLSH_FUSED_STATS
+  // instrumented builds: per-role cycle counters of the fused pass, printed to stderr
+  static unsigned long long* stats = nullptr;
+  if (!stats) CUDA_TRY(cudaMalloc(&stats, kStatCount * sizeof(unsigned long long)));
+  CUDA_TRY(cudaMemsetAsync(stats, 0, kStatCount * sizeof(unsigned long long), st));
+  f.stats = stats;
+#endif
   CUDA_TRY(launch_fused(f, st));
+#ifdef CURPLSH_FUSED_STATS
+  {
+    unsigned long long h[kStatCount];
+    CUDA_TRY(cudaMemcpyAsync(h, stats, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    const double ctas = (double)plan.grid;
+    fprintf(stderr,
+            "[fused-stats] grid %d kp %d P %d | per CTA (Mcycles): total %.2f prod_wait_empty %.2f mma_wait_full %.2f "
+            "mma_wait_acc %.2f | per epi warp: wait_acc %.2f filter %.2f refresh %.2f | refreshes %llu survivors %llu\n",
+            plan.grid, kp, P, h[kStatCtaCycles] / ctas / 1e6, h[kStatProducerWaitEmpty] / ctas / 1e6,
+            h[kStatMmaWaitFull] / ctas / 1e6, h[kStatMmaWaitAccEmpty] / ctas / 1e6,
+            h[kStatEpiWaitAccFull] / ctas / 8 / 1e6, h[kStatEpiFilter] / ctas / 8 / 1e6,
+            h[kStatEpiRefresh] / ctas / 8 / 1e6, h[kStatRefreshes], h[kStatSurvivors]);
+  }
+#endif
   tm->rec(3, st);
   MergeLaunch m{};
   m.nq = nq;

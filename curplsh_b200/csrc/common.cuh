@@ -93,6 +93,21 @@ struct FusedParams {
   int* pool_counts;        // [G*128][U][2]
   uint32_t* q_bound;       // [nq_pad] shared per-query bound (ordered bits), init kOrdInf
   uint32_t* status;        // device error word
+  unsigned long long* stats;  // per-role cycle counters, written only by builds with CURPLSH_FUSED_STATS
+};
+
+// Counter slots of FusedParams::stats (instrumented builds).
+enum FusedStat : int {
+  kStatProducerWaitEmpty = 0,  // producer lane: cycles waiting for a free stage
+  kStatMmaWaitFull,            // MMA lane: cycles waiting for TMA data
+  kStatMmaWaitAccEmpty,        // MMA lane: cycles waiting for the epilogue to free an accumulator
+  kStatEpiWaitAccFull,         // epilogue warps (lane 0): cycles waiting for an accumulator
+  kStatEpiFilter,              // epilogue warps: cycles filtering tiles
+  kStatEpiRefresh,             // epilogue warps: cycles in pool refreshes
+  kStatRefreshes,              // number of pool refreshes
+  kStatSurvivors,              // candidates appended to pools
+  kStatCtaCycles,              // sum over CTAs of kernel cycles
+  kStatCount
 };
 
 struct MergeParams {

@@ -158,6 +158,23 @@ __device__ __forceinline__ float bound_to_thr(float dstar, float qn) {
   return (dstar - qn) + (fabsf(dstar) + fabsf(qn)) * 4.76837158203125e-7f;  // 2^-21
 }
 
+// Instrumentation (compiled in only with -DCURPLSH_FUSED_STATS): per-role
+// cycle counters accumulated in registers and added to p.stats at exit.
+#ifdef CURPLSH_FUSED_STATS
+#define STAT_DECL(name) unsigned long long name = 0
+#define STAT_BEGIN(t) const long long t = clock64()
+#define STAT_END(t, acc) acc += (unsigned long long)(clock64() - t)
+#define STAT_INC(acc, v) acc += (unsigned long long)(v)
+#define STAT_FLUSH(slot, acc) \
+  if (p.stats) atomicAdd(&p.stats[slot], acc)
+#else
+#define STAT_DECL(name)
+#define STAT_BEGIN(t)
+#define STAT_END(t, acc)
+#define STAT_INC(acc, v)
+#define STAT_FLUSH(slot, acc)
+#endif
+
 // ------------------------------------------------------------------ kernel
 template <int FORM>
 __global__ void __launch_bounds__(kNumThreads, 1)
@@ -184,6 +201,7 @@ __global__ void __launch_bounds__(kNumThreads, 1)
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
+  STAT_BEGIN(t_kernel);
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
@@ -228,6 +246,7 @@ __global__ void __launch_bounds__(kNumThreads, 1)
       int qb, t0, t1, u_ord, unit = 0;
       uint32_t it = 0;
       bool ok = true;
+      STAT_DECL(st_wait);
       while (ok && walk.next(blockIdx.x, qb, t0, t1, u_ord)) {
         if (!L.a_stream) {
           if (unit > 0 && !wait_or_abort(a_empty, (unit - 1) & 1, abort_flag)) {
@@ -244,11 +263,13 @@ __global__ void __launch_bounds__(kNumThreads, 1)
         for (int t = t0; t < t1 && ok; ++t) {
           for (int kc = 0; kc < L.nkc; ++kc, ++it) {
             const int s = (int)(it % (uint32_t)S);
+            STAT_BEGIN(tw);
             if (!wait_or_abort(&empty[s], ((it / S) & 1u) ^ 1u, abort_flag)) {
               raise_abort(abort_flag, p.status, kErrWaitTimeout);
               ok = false;
               break;
             }
+            STAT_END(tw, st_wait);
             uint8_t* st = smem + L.a_bytes + (uint32_t)s * L.stage_bytes;
             mbar_arrive_expect_tx(&full[s], L.stage_bytes);
             for (int part = 0; part < Tr::kBParts; ++part)
@@ -261,6 +282,7 @@ __global__ void __launch_bounds__(kNumThreads, 1)
         }
         ++unit;
       }
+      STAT_FLUSH(kStatProducerWaitEmpty, st_wait);
     }
   } else if (warp == 1) {
     // ------------------------------------------------------------ MMA issuer
@@ -271,6 +293,8 @@ __global__ void __launch_bounds__(kNumThreads, 1)
       int qb, t0, t1, u_ord, unit = 0;
       uint32_t it = 0, tc = 0;
       bool ok = true;
+      STAT_DECL(st_full);
+      STAT_DECL(st_acc);
       while (ok && walk.next(blockIdx.x, qb, t0, t1, u_ord)) {
         if (!L.a_stream) {
           if (!wait_or_abort(a_full, unit & 1, abort_flag)) {
@@ -281,21 +305,25 @@ __global__ void __launch_bounds__(kNumThreads, 1)
         }
         for (int t = t0; t < t1 && ok; ++t, ++tc) {
           const uint32_t slot = tc & 1u, use = tc >> 1;
+          STAT_BEGIN(ta);
           if (!wait_or_abort(&acc_empty[slot], (use & 1u) ^ 1u, abort_flag)) {
             raise_abort(abort_flag, p.status, kErrWaitTimeout);
             ok = false;
             break;
           }
+          STAT_END(ta, st_acc);
           tc_fence_after();
           const uint32_t d_tmem = tmem_base + slot * kBN;
           uint32_t accumulate = 0;
           for (int kc = 0; kc < L.nkc; ++kc, ++it) {
             const int s = (int)(it % (uint32_t)S);
+            STAT_BEGIN(tf);
             if (!wait_or_abort(&full[s], (it / S) & 1u, abort_flag)) {
               raise_abort(abort_flag, p.status, kErrWaitTimeout);
               ok = false;
               break;
             }
+            STAT_END(tf, st_full);
             tc_fence_after();
             const int rem = p.d - kc * KC;
             const int nsteps = rem >= KC ? KC / Tr::kStepElems : (rem + Tr::kStepElems - 1) / Tr::kStepElems;
@@ -327,6 +355,8 @@ __global__ void __launch_bounds__(kNumThreads, 1)
       // Make sure every issued MMA has retired before TMEM is released.
       mma_commit(drain);
       mbar_wait(drain, 0);
+      STAT_FLUSH(kStatMmaWaitFull, st_full);
+      STAT_FLUSH(kStatMmaWaitAccEmpty, st_acc);
     }
   } else {
     // ------------------------------------------------------------ epilogue
@@ -342,6 +372,11 @@ __global__ void __launch_bounds__(kNumThreads, 1)
     int qb, t0, t1, u_ord;
     uint32_t tc = 0;
     bool ok = true;
+    STAT_DECL(st_wait);
+    STAT_DECL(st_filter);
+    STAT_DECL(st_refresh);
+    STAT_DECL(st_nref);
+    STAT_DECL(st_surv);
     while (ok && walk.next(blockIdx.x, qb, t0, t1, u_ord)) {
       if (u_ord < 0 || u_ord >= U) {
         raise_abort(abort_flag, p.status, kErrBadSchedule);
@@ -361,13 +396,15 @@ __global__ void __launch_bounds__(kNumThreads, 1)
       float thr = 3.402823466e38f;  // FLT_MAX: +inf norms of padding rows never pass
 
       auto refresh = [&](uint32_t need, int keep) {
+        STAT_BEGIN(tr);
+        STAT_INC(st_nref, __popc(need));
         while (need) {
           const int src = __ffs(need) - 1;
           need &= need - 1;
           const int n_src = __shfl_sync(0xffffffffu, n, src);
           int kept = 0;
           const uint64_t kmax =
-              warp_select_keep(pool_of(lg * 32 + src), n_src < P ? n_src : P, keep, hist, kept);
+              warp_select_keep_any(pool_of(lg * 32 + src), n_src < P ? n_src : P, keep, P, hist, kept);
           if (lane == src) {
             n = kept;
             const uint32_t ord = (uint32_t)(kmax >> 32);
@@ -376,6 +413,7 @@ __global__ void __launch_bounds__(kNumThreads, 1)
             if (kept >= p.kprime) atomicMin(&p.q_bound[q], ord);
           }
         }
+        STAT_END(tr, st_refresh);
       };
 
       for (int t = t0; t < t1; ++t, ++tc) {
@@ -384,11 +422,14 @@ __global__ void __launch_bounds__(kNumThreads, 1)
           const uint32_t ob = ld_relaxed_u32(&p.q_bound[q]);
           if (ob != kOrdInf) thr = fminf(thr, bound_to_thr(ord2f(ob), qn));
         }
+        STAT_BEGIN(tw);
         if (!wait_or_abort(&acc_full[slot], use & 1u, abort_flag)) {
           raise_abort(abort_flag, p.status, kErrWaitTimeout);
           ok = false;
           break;
         }
+        STAT_END(tw, st_wait);
+        STAT_BEGIN(tfl);
         tc_fence_after();
         const int colh = t * kBN + g * kHalfN;
 #pragma unroll 1
@@ -398,40 +439,48 @@ __global__ void __launch_bounds__(kNumThreads, 1)
           tmem_ld_wait();
           const int col0 = colh + c * 32;
           const float4* xn4 = reinterpret_cast<const float4*>(p.db_norms + col0);
+          // d' = ||x||^2 - 2 q.x per column; bit j of m marks a survivor
           float dd[32];
-          bool any = false;
+          uint32_t m = 0;
 #pragma unroll
           for (int j4 = 0; j4 < 8; ++j4) {
             const float4 xn = __ldg(xn4 + j4);
-            float a0 = __uint_as_float(v[4 * j4 + 0]), a1 = __uint_as_float(v[4 * j4 + 1]);
-            float a2 = __uint_as_float(v[4 * j4 + 2]), a3 = __uint_as_float(v[4 * j4 + 3]);
+            float a[4] = {__uint_as_float(v[4 * j4 + 0]), __uint_as_float(v[4 * j4 + 1]),
+                          __uint_as_float(v[4 * j4 + 2]), __uint_as_float(v[4 * j4 + 3])};
             if (Tr::kFP8) {
               const float4 sx = __ldg(reinterpret_cast<const float4*>(p.db_scale + col0) + j4);
-              a0 *= sx.x;
-              a1 *= sx.y;
-              a2 *= sx.z;
-              a3 *= sx.w;
+              a[0] *= sx.x;
+              a[1] *= sx.y;
+              a[2] *= sx.z;
+              a[3] *= sx.w;
             }
-            dd[4 * j4 + 0] = fmaf(a0, m2s, xn.x);
-            dd[4 * j4 + 1] = fmaf(a1, m2s, xn.y);
-            dd[4 * j4 + 2] = fmaf(a2, m2s, xn.z);
-            dd[4 * j4 + 3] = fmaf(a3, m2s, xn.w);
-            any |= (dd[4 * j4 + 0] <= thr) | (dd[4 * j4 + 1] <= thr) | (dd[4 * j4 + 2] <= thr) |
-                   (dd[4 * j4 + 3] <= thr);
-          }
-          if (any && valid) {
+            const float x4[4] = {xn.x, xn.y, xn.z, xn.w};
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
-              if (dd[j] <= thr) {
-                if (n < P) pool[n] = make_key(dd[j] + qn, (uint32_t)(col0 + j));
-                ++n;
-              }
+            for (int u = 0; u < 4; ++u) {
+              const int j = 4 * j4 + u;
+              dd[j] = fmaf(a[u], m2s, x4[u]);
+              m |= (dd[j] <= thr ? 1u : 0u) << j;
+            }
+          }
+          if (!valid) m = 0;
+          if (__any_sync(0xffffffffu, m != 0)) {
+            // rare path, kept compact: stash the chunk and append survivors one by one
+            float stash[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) stash[j] = dd[j];
+            while (m) {
+              const int j = __ffs(m) - 1;
+              m &= m - 1;
+              if (n < P) pool[n] = make_key(stash[j] + qn, (uint32_t)(col0 + j));
+              ++n;
+              STAT_INC(st_surv, 1);
             }
           }
         }
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(&acc_empty[slot]);
+        STAT_END(tfl, st_filter);
         if (n > P) atomicOr(p.status, kErrPoolOverflow);
         // a pool must have room for the next tile's half (kHalfN columns)
         refresh(__ballot_sync(0xffffffffu, n > P - kHalfN), p.kprime);
@@ -440,6 +489,13 @@ __global__ void __launch_bounds__(kNumThreads, 1)
       refresh(__ballot_sync(0xffffffffu, n > p.kprime), p.kprime);
       if (valid) p.pool_counts[((pool_row0 + row) * U + u_ord) * 2 + g] = n < p.kprime ? n : p.kprime;
     }
+    if (lane == 0) {
+      STAT_FLUSH(kStatEpiWaitAccFull, st_wait);
+      STAT_FLUSH(kStatEpiFilter, st_filter);
+      STAT_FLUSH(kStatEpiRefresh, st_refresh);
+      STAT_FLUSH(kStatRefreshes, st_nref);
+    }
+    STAT_FLUSH(kStatSurvivors, st_surv);
   }
 
   tc_fence_before();
@@ -448,6 +504,9 @@ __global__ void __launch_bounds__(kNumThreads, 1)
     tc_fence_after();
     tmem_dealloc(tmem_base, 512);
   }
+#ifdef CURPLSH_FUSED_STATS
+  if (threadIdx.x == 0 && p.stats) atomicAdd(&p.stats[kStatCtaCycles], (unsigned long long)(clock64() - t_kernel));
+#endif
 }
 
 // ------------------------------------------------------------------ host side
@@ -557,6 +616,7 @@ cudaError_t launch_fused(const FusedLaunch& f, cudaStream_t st) {
   p.pool_counts = f.pool_counts;
   p.q_bound = f.q_bound;
   p.status = f.status;
+  p.stats = f.stats;
   const uint32_t smem = make_layout(f.form, f.d).total;
   switch (f.form) {
     case kFormExact:

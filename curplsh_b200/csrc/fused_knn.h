@@ -35,6 +35,7 @@ struct FusedLaunch {
   int* pool_counts;
   uint32_t* q_bound;
   uint32_t* status;
+  unsigned long long* stats = nullptr;  // instrumented builds only
   FusedPlan plan;
 };
 
