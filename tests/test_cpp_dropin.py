@@ -1,0 +1,35 @@
+"""The C++ drop-in headers (include/curplsh/*.h): they compile against the C
+ABI here, and on a GPU the reference's smoke pattern runs through them."""
+import os
+import shutil
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CUDA = "/usr/local/cuda"
+
+
+def _compile(out):
+    cxx = shutil.which("g++")
+    if not cxx:
+        pytest.skip("g++ not available")
+    cmd = [cxx, "-std=c++17", "-O2", "-Wall", "-I", os.path.join(ROOT, "include"), "-I", f"{CUDA}/include",
+           os.path.join(ROOT, "tests", "cpp", "test_index_bf.cpp"), "-L", os.path.join(ROOT, "curplsh_b200"),
+           "-lcurplsh_b200", "-L", f"{CUDA}/lib64", "-lcudart", f"-Wl,-rpath,{os.path.join(ROOT, 'curplsh_b200')}",
+           "-o", out]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
+def test_cpp_headers_compile(tmp_path):
+    _compile(str(tmp_path / "t"))
+
+
+@pytest.mark.gpu
+def test_cpp_dropin_runs_reference_pattern(tmp_path):
+    exe = str(tmp_path / "t")
+    _compile(exe)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "cpp drop-in ok" in r.stdout
