@@ -64,7 +64,7 @@ def lib_path() -> str:
 
 def _load():
     if not os.path.exists(_LIB_PATH):
-        raise ImportError(f"{_LIB_PATH} is missing: run `python -m curplsh_b200.build` "
+        raise ImportError(f"{_LIB_PATH} is missing: run `python curplsh_b200/build.py` "
                           "(there is no CPU fallback)")
     lib = ctypes.CDLL(_LIB_PATH)
     vp, i32, i64, f32p, i32p = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p
@@ -95,6 +95,7 @@ def _load():
         "curplsh_index_get_device": (i32, [vp, ctypes.POINTER(ctypes.c_int)]),
         "curplsh_compute_l2_norm": (i32, [f32p, i64, i32, f32p, i32, vp]),
         "curplsh_search_l2_distance": (i32, [vp, f32p, i64, f32p, f32p, i64, i32, i32, i32p, f32p, i32]),
+        "curplsh_index_search_noalloc": (i32, [vp, i64, f32p, i32, i32p, f32p, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -115,7 +116,7 @@ EXPORTED_SYMBOLS = (
     "curplsh_index_train", "curplsh_index_add", "curplsh_index_search", "curplsh_index_search_ex",
     "curplsh_index_search_profiled", "curplsh_index_reset", "curplsh_index_get_dimension",
     "curplsh_index_get_num_data", "curplsh_index_get_device", "curplsh_compute_l2_norm",
-    "curplsh_search_l2_distance",
+    "curplsh_search_l2_distance", "curplsh_index_search_noalloc",
 )
 
 
@@ -286,6 +287,15 @@ class IndexBF:
                                                   _ptr(indices, np.int32, True), _ptr(distances, np.float32, True),
                                                   _stream_ptr(stream), ms))
         return {"prep_ms": ms[0], "fused_ms": ms[1], "merge_ms": ms[2], "total_ms": ms[3]}
+
+    def search_noalloc(self, num: int, queries, k: int, indices, distances, stream=None) -> None:
+        """Search without allocating any memory (for callers that cannot allocate
+        device memory while serving).  queries / indices / distances must be CUDA
+        tensors on the index's device; runs out of the library's fixed 64 MiB
+        scratch and returns once the results are written."""
+        _check(_lib.curplsh_index_search_noalloc(self._h, int(num), _ptr(queries, np.float32), int(k),
+                                                 _ptr(indices, np.int32, True), _ptr(distances, np.float32, True),
+                                                 _stream_ptr(stream)))
 
     def reset(self) -> None:
         _check(_lib.curplsh_index_reset(self._h))

@@ -1,7 +1,10 @@
 """Build libcurplsh_b200.so in-tree with nvcc for sm_100a (B200).
 
-    python -m curplsh_b200.build            # incremental
-    python -m curplsh_b200.build --force    # rebuild everything
+    python curplsh_b200/build.py            # incremental
+    python curplsh_b200/build.py --force    # rebuild everything
+
+Run it as a script (or load it by path, as __graft_entry__.build() does):
+importing the package itself loads the library, which may not exist yet.
 
 Objects go to curplsh_b200/_build/ (git-ignored); the shared library lands at
 curplsh_b200/libcurplsh_b200.so so that it travels with the source tree.

@@ -496,6 +496,34 @@ int do_search(curplsh_index* ix, int64_t num, const float* queries, int k, int p
 
 }  // namespace
 
+// ================================================================== internals
+namespace curplsh_b200 {
+int index_lock_view(curplsh_index* ix, IndexView* v) {
+  if (!ix || !v) return set_error(CURPLSH_ERR_INVALID_ARG, "null argument");
+  ix->mu.lock();
+  v->device = ix->cfg.device;
+  v->dim = ix->dim;
+  v->precision = ix->cfg.precision;
+  v->rerank_factor = ix->cfg.rerank_factor;
+  v->num_sms = ix->dres->num_sms;
+  v->n = ix->n;
+  v->n_pad = ix->n_pad;
+  v->ld16 = ix->ld16;
+  v->ld8 = ix->ld8;
+  v->x32 = ix->x32;
+  v->xn = ix->xn;
+  v->xh = ix->xh;
+  v->xl = ix->xl;
+  v->x8 = ix->x8;
+  v->xs = ix->xs;
+  return CURPLSH_OK;
+}
+void index_unlock(curplsh_index* ix) { ix->mu.unlock(); }
+int search_kprime(int form, int k, int rerank_factor, long long n) { return kprime_for(form, k, rerank_factor, n); }
+int search_pool_capacity(int kprime) { return pool_capacity(kprime); }
+int record_error(int code, const char* msg) { return set_error(code, "%s", msg); }
+}  // namespace curplsh_b200
+
 // ================================================================== C ABI
 extern "C" {
 

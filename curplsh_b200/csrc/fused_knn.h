@@ -71,3 +71,28 @@ cudaError_t launch_merge_rerank(const MergeLaunch& m, cudaStream_t st);
 cudaError_t launch_fill_results(int* idx, float* dist, long long n, cudaStream_t st);
 
 }  // namespace curplsh_b200
+
+// ---------------------------------------------------------------- index internals
+// Read-only view of an index's prepared database, for library code outside
+// capi.cpp (the allocation-free search).  Implemented in capi.cpp.
+struct curplsh_index;
+namespace curplsh_b200 {
+struct IndexView {
+  int device, dim, precision, rerank_factor, num_sms;
+  long long n, n_pad, ld16, ld8;
+  const float* x32;
+  const float* xn;
+  const __nv_bfloat16* xh;
+  const __nv_bfloat16* xl;
+  const uint8_t* x8;
+  const float* xs;
+};
+// Locks the index (same lock as search/add) and fills `out`; unlock with index_unlock.
+int index_lock_view(curplsh_index* index, IndexView* out);
+void index_unlock(curplsh_index* index);
+// Candidate count k' and pool capacity used by every search of this library.
+int search_kprime(int form, int k, int rerank_factor, long long n);
+int search_pool_capacity(int kprime);
+// Records a message for curplsh_last_error() and returns `code`.
+int record_error(int code, const char* msg);
+}  // namespace curplsh_b200

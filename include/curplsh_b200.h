@@ -123,6 +123,21 @@ int curplsh_index_search_ex(curplsh_index* index, int64_t num, const float* quer
 int curplsh_index_search_profiled(curplsh_index* index, int64_t num, const float* queries, int k,
                                   int precision, int rerank_factor, int* indices, float* distances,
                                   void* stream, float* pass_ms);
+/* Allocation-free search.  No counterpart in the reference: it exists for callers that cannot
+ * allocate device memory while serving (a process whose GPU memory is owned by another allocator,
+ * or a latency-critical loop where cudaMalloc/cudaFree's device-wide synchronisation is not
+ * acceptable).  Same results as curplsh_index_search_ex with the index's default precision, but
+ * the per-call working memory is a fixed 64 MiB array inside the library (held by every GPU that
+ * loads it, until exit) instead of cudaMalloc'd buffers.  queries [num x dim], indices and
+ * distances [num x k] must be device memory of the index's device; calls on one device are
+ * serialised and the call returns when the results are written (it synchronises `stream`, NULL =
+ * the legacy default stream).  The first call on a device looks up the array's device address, so
+ * make it before any stream capture.  Requests whose working set exceeds the array are rejected
+ * with CURPLSH_ERR_INVALID_ARG (roughly: num * (2*k'+128+max(k',256)) * 16 bytes must fit, k' the
+ * candidate count); an index whose FP8 copy was never built by a regular FP8 search is rejected
+ * with CURPLSH_ERR_STATE. */
+int curplsh_index_search_noalloc(curplsh_index* index, int64_t num, const float* queries, int k, int* indices,
+                                 float* distances, void* stream);
 /* Index::reset (include/index.h:56, src/index_bf.cpp:17-24) */
 int curplsh_index_reset(curplsh_index* index);
 /* getDimension / getNumData / getDevice (include/index.h:58-64) */
