@@ -305,15 +305,15 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
   uint8_t* q8 = form == kFormFP8 ? c.take<uint8_t>((size_t)nq_pad * ix->ld8) : nullptr;
   float* qn = c.take<float>(nq_pad);
   float* qs = c.take<float>(nq_pad);
-  uint32_t* qbound = c.take<uint32_t>(nq_pad);
+  uint32_t* qbound = c.take<uint32_t>(3 * nq_pad);  // [nq_pad] k'-th bounds, then [nq_pad][2] half bounds
   int* counts = c.take<int>(pool_lists);
   uint64_t* pools = c.take<uint64_t>(pool_lists * (size_t)P);
   (void)w;
 
   tm->rec(1, st);
   CUDA_TRY(launch_prep_rows(q_dev, d, nq, nq_pad, d, qn, 0.f, form == kFormFP8 ? nullptr : qh, ql, ix->ld16,
-                            q8, qs, ix->ld8, st));
-  CUDA_TRY(cudaMemsetAsync(qbound, 0xFF, (size_t)nq_pad * sizeof(uint32_t), st));
+                            q8, qs, ix->ld8, st, form == kFormFP8 ? kAugNone : kAugQuery));
+  CUDA_TRY(cudaMemsetAsync(qbound, 0xFF, (size_t)3 * nq_pad * sizeof(uint32_t), st));
   tm->rec(2, st);
   FusedLaunch f{};
   f.nq = nq;
@@ -339,6 +339,7 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
   f.pools = pools;
   f.pool_counts = counts;
   f.q_bound = qbound;
+  f.q_bound_half = qbound + nq_pad;
   f.status = ix->status;
   f.plan = plan;
 #ifdef CURPLSH_FUSED_STATS
@@ -362,6 +363,13 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
             h[kStatMmaWaitFull] / ctas / 1e6, h[kStatMmaWaitAccEmpty] / ctas / 1e6,
             h[kStatEpiWaitAccFull] / ctas / 8 / 1e6, h[kStatEpiFilter] / ctas / 8 / 1e6,
             h[kStatEpiRefresh] / ctas / 8 / 1e6, h[kStatRefreshes], h[kStatSurvivors]);
+    fprintf(stderr,
+            "[fused-stats2] radix passes/refresh %.2f | slow chunks %llu (%.1f%% of warp-chunks) | loop iters/slow "
+            "chunk %.2f | tmem Mcycles/warp %.2f\n",
+            h[kStatRefreshes] ? (double)h[kStatRadixPasses] / h[kStatRefreshes] : 0.0, h[kStatSlowChunks],
+            100.0 * h[kStatSlowChunks] / (ctas * 8 * (double)plan.work_per_cta * 4),
+            h[kStatSlowChunks] ? (double)h[kStatLoopIters] / h[kStatSlowChunks] : 0.0,
+            h[kStatTmemCycles] / ctas / 8 / 1e6);
   }
 #endif
   tm->rec(3, st);
@@ -401,7 +409,7 @@ size_t search_workspace_bytes(const curplsh_index* ix, int nq, int k, int form, 
   if (form == kFormFP8) add((size_t)nq_pad * ix->ld8);
   add(nq_pad * 4);
   add(nq_pad * 4);
-  add(nq_pad * 4);
+  add(nq_pad * 12);
   add(pool_lists * 4);
   add(pool_lists * (size_t)P * 8);
   return (size_t)round_up((long long)b, 256) + 256;
@@ -655,7 +663,7 @@ int curplsh_index_bf_create(curplsh_resources* r, int dim, const curplsh_bf_conf
   ix->dim = dim;
   ix->cfg = c;
   ix->dres = d;
-  ix->ld16 = round_up(dim, 8);
+  ix->ld16 = round_up(dim + kAugCols, 8);  // BF16 rows carry the augmented norm columns
   ix->ld8 = round_up(dim, 16);
   r->refs.fetch_add(1);
   DeviceScope scope(c.device);
@@ -737,7 +745,7 @@ int curplsh_index_add(curplsh_index* ix, int64_t num, const float* data) {
   const float inf = __builtin_huge_valf();
   CUDA_TRY(launch_prep_rows(x32 + (size_t)n_old * d, d, (int)num, pad_new - n_old, d, xn + n_old, inf,
                             xh + (size_t)n_old * ix->ld16, xl + (size_t)n_old * ix->ld16, ix->ld16, nullptr,
-                            nullptr, ix->ld8, st));
+                            nullptr, ix->ld8, st, kAugDatabase));
   CUDA_TRY(cudaStreamSynchronize(st));
   // swap in
   float* old_x32 = ix->x32;

@@ -68,6 +68,11 @@ constexpr int kBN = 256;          // database rows per tile: MMA N (TMEM columns
 constexpr int kHalfN = kBN / 2;   // columns of a tile handled by one epilogue warpgroup
 constexpr int kChunkBytes = 128;  // K extent of one smem chunk row (one 128-byte swizzle atom)
 constexpr int kNumThreads = 320;  // warp 0 TMA producer, warp 1 MMA issuer, warps 2..9 epilogue
+// BF16 forms append kAugCols columns to every row so the tensor cores add the
+// norms: database rows carry [n1 n2 n3 1 1 1] (||x||^2 = n1+n2+n3, three BF16
+// terms), query rows (stored as -2q) carry [1 1 1 m1 m2 m3] (||q||^2 = m1+m2+m3),
+// and the accumulator is ||q||^2 + ||x||^2 - 2 q.x directly.
+constexpr int kAugCols = 6;
 constexpr int kEpiWarps = 8;
 
 struct FusedParams {
@@ -92,6 +97,7 @@ struct FusedParams {
   uint64_t* pools;         // [G*128][U][2][pool_cap]
   int* pool_counts;        // [G*128][U][2]
   uint32_t* q_bound;       // [nq_pad] shared per-query bound (ordered bits), init kOrdInf
+  uint32_t* q_bound_half;  // [nq_pad][2] per-query, per-half (k'/2)-th bounds, init kOrdInf
   uint32_t* status;        // device error word
   unsigned long long* stats;  // per-role cycle counters, written only by builds with CURPLSH_FUSED_STATS
 };
@@ -107,6 +113,10 @@ enum FusedStat : int {
   kStatRefreshes,              // number of pool refreshes
   kStatSurvivors,              // candidates appended to pools
   kStatCtaCycles,              // sum over CTAs of kernel cycles
+  kStatRadixPasses,            // histogram passes run by pool refreshes
+  kStatSlowChunks,             // warp-chunks (32 columns) that entered the survivor path
+  kStatLoopIters,              // survivor-append loop iterations executed by warps
+  kStatTmemCycles,             // epilogue warps (lane 0): cycles in TMEM loads + waits
   kStatCount
 };
 

@@ -46,6 +46,7 @@ struct FormTraits<kFormExact> {
   static constexpr int kAParts = 2, kBParts = 2, kProducts = 3;
   static constexpr int kChunkElems = 64, kStepElems = 16;  // bf16
   static constexpr bool kFP8 = false;
+  static constexpr bool kFolded = true;  // norms ride in the augmented K columns
   // products: hi*hi, hi*lo, lo*hi  (the lo*lo term, O(2^-16) relative, is dropped)
   __device__ static constexpr int a_part(int p) { return p == 2 ? 1 : 0; }
   __device__ static constexpr int b_part(int p) { return p == 1 ? 1 : 0; }
@@ -55,6 +56,7 @@ struct FormTraits<kFormBF16> {
   static constexpr int kAParts = 1, kBParts = 1, kProducts = 1;
   static constexpr int kChunkElems = 64, kStepElems = 16;
   static constexpr bool kFP8 = false;
+  static constexpr bool kFolded = true;
   __device__ static constexpr int a_part(int) { return 0; }
   __device__ static constexpr int b_part(int) { return 0; }
 };
@@ -63,16 +65,24 @@ struct FormTraits<kFormFP8> {
   static constexpr int kAParts = 1, kBParts = 1, kProducts = 1;
   static constexpr int kChunkElems = 128, kStepElems = 32;  // e4m3
   static constexpr bool kFP8 = true;
+  static constexpr bool kFolded = false;  // per-row scales: norms are applied in the epilogue
   __device__ static constexpr int a_part(int) { return 0; }
   __device__ static constexpr int b_part(int) { return 0; }
 };
 
 constexpr uint32_t kAChunkBytes = kBM * kChunkBytes;  // 16 KB
 constexpr uint32_t kBChunkBytes = kBN * kChunkBytes;  // 32 KB
+// A narrow tail chunk holds the last <= 16 BF16 columns (the augmented norm
+// columns when d is a multiple of 64): 32-byte rows, 32-byte swizzle.
+constexpr uint32_t kTailRowBytes = 32;
+constexpr uint32_t kATailBytes = kBM * kTailRowBytes;  // 4 KB
+constexpr uint32_t kBTailBytes = kBN * kTailRowBytes;  // 8 KB
 
 // ------------------------------------------------------------------ smem layout
 struct SmemLayout {
-  int nkc;             // K chunks (128 bytes of K each)
+  int kdim;            // K extent of the MMA (d, plus kAugCols for the folded forms)
+  int nkc;             // K chunks (128 bytes of K each, except a narrow tail)
+  int tail_narrow;     // 1: the last chunk is a 16-column, 32-byte-swizzled tail
   int a_stream;        // 1: query chunks travel with each stage
   uint32_t a_bytes;    // resident query block bytes (0 when streamed)
   uint32_t stage_bytes;
@@ -84,28 +94,53 @@ struct SmemLayout {
 
 __host__ __device__ inline SmemLayout make_layout(int form, int d) {
   SmemLayout L{};
-  const int chunk_elems = (form == kFormFP8) ? 128 : 64;
+  const bool folded = form != kFormFP8;
+  const int chunk_elems = folded ? 64 : 128;
   const int a_parts = (form == kFormExact) ? 2 : 1;
   const int b_parts = (form == kFormExact) ? 2 : 1;
-  L.nkc = (d + chunk_elems - 1) / chunk_elems;
-  const uint32_t budget = 200u * 1024u;
-  const uint32_t a_res = (uint32_t)L.nkc * a_parts * kAChunkBytes;
-  const uint32_t b_stage = (uint32_t)b_parts * kBChunkBytes;
-  if (a_res + 2 * b_stage <= budget) {
+  L.kdim = folded ? d + kAugCols : d;
+  L.nkc = (L.kdim + chunk_elems - 1) / chunk_elems;
+  // narrow tail only when it holds nothing but the norm columns (d % 64 == 0):
+  // the tail runs the hi x hi product alone, which is exact only for those
+  L.tail_narrow = folded && (d % 64 == 0);
+  // everything below the barrier block must fit the 227 KB opt-in limit
+  const uint32_t budget = 227u * 1024u - 256u - (uint32_t)kEpiWarps * 256u * 4u - 1024u;
+  const int nreg = L.nkc - (L.tail_narrow ? 1 : 0);
+  const uint32_t a_res = (uint32_t)nreg * a_parts * kAChunkBytes + (L.tail_narrow ? kATailBytes : 0u);
+  // a stage = one regular K chunk of the tile; the last one also carries the tail
+  const uint32_t b_stage = (uint32_t)b_parts * kBChunkBytes + (L.tail_narrow ? kBTailBytes : 0u);
+  if (((a_res + 1023u) & ~1023u) + 2 * b_stage <= budget) {
     L.a_stream = 0;
-    L.a_bytes = a_res;
+    L.a_bytes = (a_res + 1023u) & ~1023u;
     L.stage_bytes = b_stage;
   } else {
     L.a_stream = 1;
     L.a_bytes = 0;
-    L.stage_bytes = b_stage + (uint32_t)a_parts * kAChunkBytes;
+    L.stage_bytes = b_stage + (uint32_t)a_parts * kAChunkBytes + (L.tail_narrow ? kATailBytes : 0u);
   }
+  L.stage_bytes = (L.stage_bytes + 1023u) & ~1023u;
   int s = (int)((budget - L.a_bytes) / L.stage_bytes);
   L.stages = s < 2 ? 2 : (s > 8 ? 8 : s);
   L.bar_off = L.a_bytes + (uint32_t)L.stages * L.stage_bytes;
   L.hist_off = L.bar_off + 256;  // barriers: 2*8 + 6 mbarriers + tmem slot + flags < 256 B
   L.total = L.hist_off + kEpiWarps * 256 * 4 + 1024;
   return L;
+}
+
+// Offset of resident query chunk `kc`, part `part` (0 hi, 1 lo); the narrow
+// tail (kc = nkc-1) has a part 0 only.
+__device__ __forceinline__ uint32_t a_res_off(const SmemLayout& L, int kc, int part, int a_parts) {
+  return (uint32_t)(kc * a_parts + part) * kAChunkBytes;
+}
+
+// Offsets inside a stage: B parts, then streamed A parts, then the tail (B, A).
+template <int kAP, int kBP>
+__device__ __forceinline__ uint32_t stage_a_off(int part) {
+  return (uint32_t)kBP * kBChunkBytes + (uint32_t)part * kAChunkBytes;
+}
+template <int kAP, int kBP>
+__device__ __forceinline__ uint32_t stage_tail_off(const SmemLayout& L) {
+  return (uint32_t)kBP * kBChunkBytes + (L.a_stream ? (uint32_t)kAP * kAChunkBytes : 0u);
 }
 
 // ------------------------------------------------------------------ schedule
@@ -158,6 +193,14 @@ __device__ __forceinline__ float bound_to_thr(float dstar, float qn) {
   return (dstar - qn) + (fabsf(dstar) + fabsf(qn)) * 4.76837158203125e-7f;  // 2^-21
 }
 
+// Filter threshold for a bound `dstar` on the key distance.  The folded forms
+// compare the accumulator, which is the key distance itself, so the bound is
+// used as is; the FP8 form compares ||x||^2 - 2 q.x and needs bound_to_thr.
+template <bool kFolded>
+__device__ __forceinline__ float thr_from(float dstar, float qn) {
+  return kFolded ? dstar : bound_to_thr(dstar, qn);
+}
+
 // Instrumentation (compiled in only with -DCURPLSH_FUSED_STATS): per-role
 // cycle counters accumulated in registers and added to p.stats at exit.
 #ifdef CURPLSH_FUSED_STATS
@@ -175,11 +218,26 @@ __device__ __forceinline__ float bound_to_thr(float dstar, float qn) {
 #define STAT_FLUSH(slot, acc)
 #endif
 
+// v[j] for a runtime j in [0, 32) without local memory: a 5-level select tree.
+__device__ __forceinline__ float select32(const float (&v)[32], int j) {
+  float a[16], b[8], c[4], d2[2];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) a[i] = (j & 16) ? v[i + 16] : v[i];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) b[i] = (j & 8) ? a[i + 8] : a[i];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) c[i] = (j & 4) ? b[i + 4] : b[i];
+#pragma unroll
+  for (int i = 0; i < 2; ++i) d2[i] = (j & 2) ? c[i + 2] : c[i];
+  return (j & 1) ? d2[1] : d2[0];
+}
+
 // ------------------------------------------------------------------ kernel
 template <int FORM>
 __global__ void __launch_bounds__(kNumThreads, 1)
     fused_knn_kernel(const __grid_constant__ CUtensorMap tm_q_hi, const __grid_constant__ CUtensorMap tm_q_lo,
                      const __grid_constant__ CUtensorMap tm_x_hi, const __grid_constant__ CUtensorMap tm_x_lo,
+                     const __grid_constant__ CUtensorMap tm_q_tail, const __grid_constant__ CUtensorMap tm_x_tail,
                      const FusedParams p) {
   using Tr = FormTraits<FORM>;
   extern __shared__ uint8_t smem_raw[];
@@ -254,14 +312,19 @@ __global__ void __launch_bounds__(kNumThreads, 1)
             ok = false;
             break;
           }
-          mbar_arrive_expect_tx(a_full, L.a_bytes);
-          for (int kc = 0; kc < L.nkc; ++kc)
+          const int nreg = L.nkc - (L.tail_narrow ? 1 : 0);
+          mbar_arrive_expect_tx(a_full, (uint32_t)nreg * Tr::kAParts * kAChunkBytes +
+                                            (L.tail_narrow ? kATailBytes : 0u));
+          for (int kc = 0; kc < nreg; ++kc)
             for (int part = 0; part < Tr::kAParts; ++part)
-              tma_load_2d(smem + (kc * Tr::kAParts + part) * kAChunkBytes, part ? &tm_q_lo : &tm_q_hi, a_full,
+              tma_load_2d(smem + a_res_off(L, kc, part, Tr::kAParts), part ? &tm_q_lo : &tm_q_hi, a_full,
                           kc * KC, qb * kBM, pol_q);
+          if (L.tail_narrow)
+            tma_load_2d(smem + a_res_off(L, nreg, 0, Tr::kAParts), &tm_q_tail, a_full, nreg * KC, qb * kBM, pol_q);
         }
+        const int nreg = L.nkc - (L.tail_narrow ? 1 : 0);
         for (int t = t0; t < t1 && ok; ++t) {
-          for (int kc = 0; kc < L.nkc; ++kc, ++it) {
+          for (int kc = 0; kc < nreg; ++kc, ++it) {
             const int s = (int)(it % (uint32_t)S);
             STAT_BEGIN(tw);
             if (!wait_or_abort(&empty[s], ((it / S) & 1u) ^ 1u, abort_flag)) {
@@ -271,13 +334,21 @@ __global__ void __launch_bounds__(kNumThreads, 1)
             }
             STAT_END(tw, st_wait);
             uint8_t* st = smem + L.a_bytes + (uint32_t)s * L.stage_bytes;
-            mbar_arrive_expect_tx(&full[s], L.stage_bytes);
+            const bool with_tail = L.tail_narrow && kc == nreg - 1;
+            uint32_t tx = (uint32_t)Tr::kBParts * kBChunkBytes + (L.a_stream ? (uint32_t)Tr::kAParts * kAChunkBytes : 0u);
+            if (with_tail) tx += kBTailBytes + (L.a_stream ? kATailBytes : 0u);
+            mbar_arrive_expect_tx(&full[s], tx);
             for (int part = 0; part < Tr::kBParts; ++part)
               tma_load_2d(st + part * kBChunkBytes, part ? &tm_x_lo : &tm_x_hi, &full[s], kc * KC, t * kBN, pol_db);
             if (L.a_stream)
               for (int part = 0; part < Tr::kAParts; ++part)
-                tma_load_2d(st + Tr::kBParts * kBChunkBytes + part * kAChunkBytes, part ? &tm_q_lo : &tm_q_hi,
-                            &full[s], kc * KC, qb * kBM, pol_q);
+                tma_load_2d(st + stage_a_off<Tr::kAParts, Tr::kBParts>(part), part ? &tm_q_lo : &tm_q_hi, &full[s],
+                            kc * KC, qb * kBM, pol_q);
+            if (with_tail) {
+              uint8_t* tl = st + stage_tail_off<Tr::kAParts, Tr::kBParts>(L);
+              tma_load_2d(tl, &tm_x_tail, &full[s], nreg * KC, t * kBN, pol_db);
+              if (L.a_stream) tma_load_2d(tl + kBTailBytes, &tm_q_tail, &full[s], nreg * KC, qb * kBM, pol_q);
+            }
           }
         }
         ++unit;
@@ -315,7 +386,8 @@ __global__ void __launch_bounds__(kNumThreads, 1)
           tc_fence_after();
           const uint32_t d_tmem = tmem_base + slot * kBN;
           uint32_t accumulate = 0;
-          for (int kc = 0; kc < L.nkc; ++kc, ++it) {
+          const int nreg = L.nkc - (L.tail_narrow ? 1 : 0);
+          for (int kc = 0; kc < nreg; ++kc, ++it) {
             const int s = (int)(it % (uint32_t)S);
             STAT_BEGIN(tf);
             if (!wait_or_abort(&full[s], (it / S) & 1u, abort_flag)) {
@@ -325,14 +397,13 @@ __global__ void __launch_bounds__(kNumThreads, 1)
             }
             STAT_END(tf, st_full);
             tc_fence_after();
-            const int rem = p.d - kc * KC;
-            const int nsteps = rem >= KC ? KC / Tr::kStepElems : (rem + Tr::kStepElems - 1) / Tr::kStepElems;
             const uint32_t st = smem_u32(smem + L.a_bytes + (uint32_t)s * L.stage_bytes);
+            const int rem = L.kdim - kc * KC;
+            const int nsteps = rem >= KC ? KC / Tr::kStepElems : (rem + Tr::kStepElems - 1) / Tr::kStepElems;
 #pragma unroll
             for (int pr = 0; pr < Tr::kProducts; ++pr) {
-              const uint32_t a_addr =
-                  L.a_stream ? st + Tr::kBParts * kBChunkBytes + Tr::a_part(pr) * kAChunkBytes
-                             : smem_u32(smem + (kc * Tr::kAParts + Tr::a_part(pr)) * kAChunkBytes);
+              const uint32_t a_addr = L.a_stream ? st + stage_a_off<Tr::kAParts, Tr::kBParts>(Tr::a_part(pr))
+                                                 : smem_u32(smem + a_res_off(L, kc, Tr::a_part(pr), Tr::kAParts));
               const uint32_t b_addr = st + Tr::b_part(pr) * kBChunkBytes;
               for (int ks = 0; ks < nsteps; ++ks) {
                 const uint64_t ad = sw128_kmajor_desc(a_addr + ks * 32);
@@ -343,6 +414,13 @@ __global__ void __launch_bounds__(kNumThreads, 1)
                   mma_f16_ss(d_tmem, ad, bd, idesc, accumulate);
                 accumulate = 1;
               }
+            }
+            if (L.tail_narrow && kc == nreg - 1) {
+              // the 16 norm columns: only hi x hi carries them (lo rows are zero
+              // there), so one K step of product 0 with the 32-byte-swizzled tiles
+              const uint32_t tl = st + stage_tail_off<Tr::kAParts, Tr::kBParts>(L);
+              const uint32_t a_addr = L.a_stream ? tl + kBTailBytes : smem_u32(smem + a_res_off(L, nreg, 0, Tr::kAParts));
+              mma_f16_ss(d_tmem, sw32_kmajor_desc(a_addr), sw32_kmajor_desc(tl), idesc, 1);
             }
             mma_commit(&empty[s]);
           }
@@ -377,6 +455,12 @@ __global__ void __launch_bounds__(kNumThreads, 1)
     STAT_DECL(st_refresh);
     STAT_DECL(st_nref);
     STAT_DECL(st_surv);
+    STAT_DECL(st_slow);
+    STAT_DECL(st_iters);
+    STAT_DECL(st_tmem);
+#ifdef CURPLSH_FUSED_STATS
+    if (threadIdx.x == 64 && p.stats) g_radix_pass_counter = &p.stats[kStatRadixPasses];
+#endif
     while (ok && walk.next(blockIdx.x, qb, t0, t1, u_ord)) {
       if (u_ord < 0 || u_ord >= U) {
         raise_abort(abort_flag, p.status, kErrBadSchedule);
@@ -393,8 +477,14 @@ __global__ void __launch_bounds__(kNumThreads, 1)
       };
       uint64_t* pool = pool_of(row);
       int n = 0;
-      float thr = 3.402823466e38f;  // FLT_MAX: +inf norms of padding rows never pass
+      float thr = 3.402823466e38f;  // FLT_MAX: admits every finite distance until a pool fills
 
+      // Bounds shared between pools of this query: q_bound holds the smallest
+      // k'-th key distance any pool has reached; q_bound_half[2q+h] the
+      // smallest (k'/2)-th of any pool of half h.  Pools of different halves
+      // cover disjoint rows, so max(half 0, half 1) bounds the k'-th of their
+      // union -- about as tight as one pool over both halves.
+      uint32_t* qbh = p.q_bound_half + 2 * (size_t)(valid ? q : 0);
       auto refresh = [&](uint32_t need, int keep) {
         STAT_BEGIN(tr);
         STAT_INC(st_nref, __popc(need));
@@ -403,24 +493,41 @@ __global__ void __launch_bounds__(kNumThreads, 1)
           need &= need - 1;
           const int n_src = __shfl_sync(0xffffffffu, n, src);
           int kept = 0;
+          uint64_t half_key = 0;
           const uint64_t kmax =
-              warp_select_keep_any(pool_of(lg * 32 + src), n_src < P ? n_src : P, keep, P, hist, kept);
+              warp_select_keep_any(pool_of(lg * 32 + src), n_src < P ? n_src : P, keep, P, hist, kept, half_key);
           if (lane == src) {
             n = kept;
             const uint32_t ord = (uint32_t)(kmax >> 32);
-            thr = fminf(thr, bound_to_thr(ord2f(ord), qn));
+            thr = fminf(thr, thr_from<Tr::kFolded>(ord2f(ord), qn));
             // only a full set of k' keys bounds the global k'-th distance
-            if (kept >= p.kprime) atomicMin(&p.q_bound[q], ord);
+            if (kept >= p.kprime) {
+              atomicMin(&p.q_bound[q], ord);
+              atomicMin(&qbh[g], (uint32_t)(half_key >> 32));
+            }
           }
         }
         STAT_END(tr, st_refresh);
       };
 
+      // shared bounds are L2 round trips: load them one tile ahead
+      uint32_t nb_ob = kOrdInf, nb_h0 = kOrdInf, nb_h1 = kOrdInf;
+      if (valid) {
+        nb_ob = ld_relaxed_u32(&p.q_bound[q]);
+        nb_h0 = ld_relaxed_u32(&qbh[0]);
+        nb_h1 = ld_relaxed_u32(&qbh[1]);
+      }
       for (int t = t0; t < t1; ++t, ++tc) {
         const uint32_t slot = tc & 1u, use = tc >> 1;
-        if (valid) {
-          const uint32_t ob = ld_relaxed_u32(&p.q_bound[q]);
-          if (ob != kOrdInf) thr = fminf(thr, bound_to_thr(ord2f(ob), qn));
+        {
+          const uint32_t hb = nb_h0 > nb_h1 ? nb_h0 : nb_h1;  // both halves reported (else kOrdInf)
+          const uint32_t b = nb_ob < hb ? nb_ob : hb;
+          if (b != kOrdInf) thr = fminf(thr, thr_from<Tr::kFolded>(ord2f(b), qn));
+          if (valid) {
+            nb_ob = ld_relaxed_u32(&p.q_bound[q]);
+            nb_h0 = ld_relaxed_u32(&qbh[0]);
+            nb_h1 = ld_relaxed_u32(&qbh[1]);
+          }
         }
         STAT_BEGIN(tw);
         if (!wait_or_abort(&acc_full[slot], use & 1u, abort_flag)) {
@@ -433,47 +540,100 @@ __global__ void __launch_bounds__(kNumThreads, 1)
         tc_fence_after();
         const int colh = t * kBN + g * kHalfN;
 #pragma unroll 1
-        for (int c = 0; c < kHalfN / 32; ++c) {
-          uint32_t v[32];
-          tmem_ld_32x32b_x32(tmem_base + lane_base + slot * kBN + g * kHalfN + c * 32, v);
+        for (int h = 0; h < kHalfN / 64; ++h) {
+          uint32_t v[64];
+          STAT_BEGIN(ttm);
+          tmem_ld_32x32b_x64(tmem_base + lane_base + slot * kBN + g * kHalfN + h * 64, v);
           tmem_ld_wait();
-          const int col0 = colh + c * 32;
-          const float4* xn4 = reinterpret_cast<const float4*>(p.db_norms + col0);
-          // d' = ||x||^2 - 2 q.x per column; bit j of m marks a survivor
-          float dd[32];
-          uint32_t m = 0;
+          STAT_END(ttm, st_tmem);
 #pragma unroll
-          for (int j4 = 0; j4 < 8; ++j4) {
-            const float4 xn = __ldg(xn4 + j4);
-            float a[4] = {__uint_as_float(v[4 * j4 + 0]), __uint_as_float(v[4 * j4 + 1]),
-                          __uint_as_float(v[4 * j4 + 2]), __uint_as_float(v[4 * j4 + 3])};
-            if (Tr::kFP8) {
-              const float4 sx = __ldg(reinterpret_cast<const float4*>(p.db_scale + col0) + j4);
-              a[0] *= sx.x;
-              a[1] *= sx.y;
-              a[2] *= sx.z;
-              a[3] *= sx.w;
+          for (int cc = 0; cc < 2; ++cc) {
+            const int col0 = colh + h * 64 + cc * 32;
+            const uint32_t* vc = v + cc * 32;
+            // coarse distance per column; bit j of m marks a survivor
+            float dd[32];
+            if (Tr::kFolded) {
+              // the accumulator already is ||q||^2 + ||x||^2 - 2 q.x
+#pragma unroll
+              for (int j = 0; j < 32; ++j) dd[j] = __uint_as_float(vc[j]);
+            } else {
+              const float4* xn4 = reinterpret_cast<const float4*>(p.db_norms + col0);
+              const float4* sx4 = reinterpret_cast<const float4*>(p.db_scale + col0);
+#pragma unroll
+              for (int j4 = 0; j4 < 8; ++j4) {
+                const float4 xn = __ldg(xn4 + j4);
+                const float4 sx = __ldg(sx4 + j4);
+                dd[4 * j4 + 0] = fmaf(__uint_as_float(vc[4 * j4 + 0]) * sx.x, m2s, xn.x);
+                dd[4 * j4 + 1] = fmaf(__uint_as_float(vc[4 * j4 + 1]) * sx.y, m2s, xn.y);
+                dd[4 * j4 + 2] = fmaf(__uint_as_float(vc[4 * j4 + 2]) * sx.z, m2s, xn.z);
+                dd[4 * j4 + 3] = fmaf(__uint_as_float(vc[4 * j4 + 3]) * sx.w, m2s, xn.w);
+              }
             }
-            const float x4[4] = {xn.x, xn.y, xn.z, xn.w};
+            // quick reject: chunk minimum by a shallow three-input-min tree
+            float mn;
+            {
+              float t[11];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              const int j = 4 * j4 + u;
-              dd[j] = fmaf(a[u], m2s, x4[u]);
-              m |= (dd[j] <= thr ? 1u : 0u) << j;
+              for (int i = 0; i < 10; ++i) t[i] = fmin3(dd[3 * i], dd[3 * i + 1], dd[3 * i + 2]);
+              t[10] = fminf(dd[30], dd[31]);
+              const float u0 = fmin3(t[0], t[1], t[2]), u1 = fmin3(t[3], t[4], t[5]);
+              const float u2 = fmin3(t[6], t[7], t[8]), u3 = fminf(t[9], t[10]);
+              mn = fminf(fminf(u0, u1), fminf(u2, u3));
             }
-          }
-          if (!valid) m = 0;
-          if (__any_sync(0xffffffffu, m != 0)) {
-            // rare path, kept compact: stash the chunk and append survivors one by one
-            float stash[32];
+            const bool hit = valid && mn <= thr;
+            if (__any_sync(0xffffffffu, hit)) {
+              uint32_t m = 0;
+              if (hit) {
+                // survivor mask, OR-combined in four independent partial masks
+                uint32_t pm[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
-            for (int j = 0; j < 32; ++j) stash[j] = dd[j];
-            while (m) {
-              const int j = __ffs(m) - 1;
-              m &= m - 1;
-              if (n < P) pool[n] = make_key(stash[j] + qn, (uint32_t)(col0 + j));
-              ++n;
-              STAT_INC(st_surv, 1);
+                for (int j = 0; j < 32; ++j) pm[j & 3] |= (dd[j] <= thr ? 1u : 0u) << j;
+                m = (pm[0] | pm[1]) | (pm[2] | pm[3]);
+                // database rows beyond nb (padding of the last tile) never survive
+                if (col0 + 32 > p.nb) m &= col0 >= p.nb ? 0u : ((1u << (p.nb - col0)) - 1u);
+              }
+              if (__any_sync(0xffffffffu, m != 0)) {
+                STAT_INC(st_slow, 1);
+#ifdef CURPLSH_FUSED_STATS
+                {
+                  int mx = __popc(m);
+#pragma unroll
+                  for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+                  STAT_INC(st_iters, mx);
+                }
+#endif
+                // A lane rarely has more than two survivors in 32 columns: fetch
+                // them from registers with a select tree (no local memory), and
+                // only stash the chunk when there are more.
+                if (m) {
+                  const int j1 = __ffs(m) - 1;
+                  m &= m - 1;
+                  const float v1 = select32(dd, j1);
+                  if (n < P) pool[n] = make_key(Tr::kFolded ? v1 : v1 + qn, (uint32_t)(col0 + j1));
+                  ++n;
+                  STAT_INC(st_surv, 1);
+                }
+                if (m) {
+                  const int j2 = __ffs(m) - 1;
+                  m &= m - 1;
+                  const float v2 = select32(dd, j2);
+                  if (n < P) pool[n] = make_key(Tr::kFolded ? v2 : v2 + qn, (uint32_t)(col0 + j2));
+                  ++n;
+                  STAT_INC(st_surv, 1);
+                }
+                if (__any_sync(0xffffffffu, m != 0)) {
+                  float stash[32];
+#pragma unroll
+                  for (int j = 0; j < 32; ++j) stash[j] = dd[j];
+                  while (m) {
+                    const int j = __ffs(m) - 1;
+                    m &= m - 1;
+                    if (n < P) pool[n] = make_key(Tr::kFolded ? stash[j] : stash[j] + qn, (uint32_t)(col0 + j));
+                    ++n;
+                    STAT_INC(st_surv, 1);
+                  }
+                }
+              }
             }
           }
         }
@@ -487,13 +647,18 @@ __global__ void __launch_bounds__(kNumThreads, 1)
       }
       if (!ok) break;
       refresh(__ballot_sync(0xffffffffu, n > p.kprime), p.kprime);
-      if (valid) p.pool_counts[((pool_row0 + row) * U + u_ord) * 2 + g] = n < p.kprime ? n : p.kprime;
+      // a refresh may keep a few more than k' keys (unsorted): record them all;
+      // the merge pass selects exactly
+      if (valid) p.pool_counts[((pool_row0 + row) * U + u_ord) * 2 + g] = n < P ? n : P;
     }
     if (lane == 0) {
       STAT_FLUSH(kStatEpiWaitAccFull, st_wait);
       STAT_FLUSH(kStatEpiFilter, st_filter);
       STAT_FLUSH(kStatEpiRefresh, st_refresh);
       STAT_FLUSH(kStatRefreshes, st_nref);
+      STAT_FLUSH(kStatSlowChunks, st_slow);
+      STAT_FLUSH(kStatLoopIters, st_iters);
+      STAT_FLUSH(kStatTmemCycles, st_tmem);
     }
     STAT_FLUSH(kStatSurvivors, st_surv);
   }
@@ -528,19 +693,21 @@ EncodeTiledFn get_encode_fn() {
   return fn;
 }
 
-// 2-D K-major operand map: rows x ld elements, box = (128 bytes of K) x box_rows,
-// 128-byte swizzle, zero fill out of bounds.
-bool make_map(CUtensorMap* m, const void* base, bool fp8, long long rows, long long ld_elems, int box_rows) {
+// 2-D K-major operand map: rows x ld elements, box = (128 bytes of K) x box_rows
+// with the 128-byte swizzle, or (narrow) 32 bytes of K with the 32-byte
+// swizzle; zero fill out of bounds.
+bool make_map(CUtensorMap* m, const void* base, bool fp8, long long rows, long long ld_elems, int box_rows,
+              bool narrow = false) {
   EncodeTiledFn fn = get_encode_fn();
   if (!fn) return false;
   const int esz = fp8 ? 1 : 2;
   cuuint64_t dims[2] = {(cuuint64_t)ld_elems, (cuuint64_t)rows};
   cuuint64_t strides[1] = {(cuuint64_t)(ld_elems * esz)};
-  cuuint32_t box[2] = {(cuuint32_t)(kChunkBytes / esz), (cuuint32_t)box_rows};
+  cuuint32_t box[2] = {(cuuint32_t)((narrow ? kTailRowBytes : kChunkBytes) / esz), (cuuint32_t)box_rows};
   cuuint32_t estr[2] = {1, 1};
   CUresult r = fn(m, fp8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
                   const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  narrow ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
@@ -556,7 +723,7 @@ cudaError_t launch_form(const FusedLaunch& f, const FusedParams& p, int grid, ui
     if (e != cudaSuccess) return e;
     attr_done[dev & 15] = true;
   }
-  CUtensorMap mqh, mql, mxh, mxl;
+  CUtensorMap mqh, mql, mxh, mxl, mqt, mxt;
   const bool fp8 = FORM == kFormFP8;
   const void* qh = fp8 ? (const void*)f.q8 : (const void*)f.qh;
   const void* xh = fp8 ? (const void*)f.x8 : (const void*)f.xh;
@@ -570,7 +737,15 @@ cudaError_t launch_form(const FusedLaunch& f, const FusedParams& p, int grid, ui
     mql = mqh;
     mxl = mxh;
   }
-  fused_knn_kernel<FORM><<<grid, kNumThreads, smem, st>>>(mqh, mql, mxh, mxl, p);
+  if (FORM != kFormFP8) {
+    if (!make_map(&mqt, f.qh, false, f.nq_pad, f.ld16, kBM, true) ||
+        !make_map(&mxt, f.xh, false, f.nb_pad, f.ld16, kBN, true))
+      return cudaErrorInvalidValue;
+  } else {
+    mqt = mqh;
+    mxt = mxh;
+  }
+  fused_knn_kernel<FORM><<<grid, kNumThreads, smem, st>>>(mqh, mql, mxh, mxl, mqt, mxt, p);
   return cudaGetLastError();
 }
 
@@ -615,6 +790,7 @@ cudaError_t launch_fused(const FusedLaunch& f, cudaStream_t st) {
   p.pools = f.pools;
   p.pool_counts = f.pool_counts;
   p.q_bound = f.q_bound;
+  p.q_bound_half = f.q_bound_half;
   p.status = f.status;
   p.stats = f.stats;
   const uint32_t smem = make_layout(f.form, f.d).total;

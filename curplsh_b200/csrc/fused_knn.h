@@ -34,6 +34,7 @@ struct FusedLaunch {
   uint64_t* pools;
   int* pool_counts;
   uint32_t* q_bound;
+  uint32_t* q_bound_half;  // [nq_pad][2]
   uint32_t* status;
   unsigned long long* stats = nullptr;  // instrumented builds only
   FusedPlan plan;
@@ -45,10 +46,14 @@ cudaError_t launch_fused(const FusedLaunch& f, cudaStream_t st);
 
 // Row preparation: squared norms (FP32), BF16 hi/lo split, FP8-E4M3 with a
 // per-row FP32 scale.  Rows in [nrows, nrows_pad) are written as zeros with
-// norm `pad_norm`.  Any of the output pointers may be null.
+// norm `pad_norm`.  Any of the output pointers may be null.  `aug` selects the
+// augmented BF16 row layout (kAugNone / kAugDatabase / kAugQuery, see kAugCols):
+// database rows get [n1 n2 n3 1 1 1] after column d, query rows are stored as -2q
+// followed by [1 1 1 m1 m2 m3]; lo rows get zeros there.
+enum AugMode : int { kAugNone = 0, kAugDatabase = 1, kAugQuery = 2 };
 cudaError_t launch_prep_rows(const float* x, long long ldx, int nrows, long long nrows_pad, int d, float* norms,
                              float pad_norm, __nv_bfloat16* hi, __nv_bfloat16* lo, long long ld16, uint8_t* f8,
-                             float* scale, long long ld8, cudaStream_t st);
+                             float* scale, long long ld8, cudaStream_t st, int aug = kAugNone);
 
 // Plain squared (or not) L2 norms, as computeL2Norm.
 cudaError_t launch_l2_norms(const float* x, long long n, int d, float* norms, int squared, cudaStream_t st);

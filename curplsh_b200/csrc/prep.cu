@@ -36,10 +36,23 @@ __device__ __forceinline__ uint8_t to_e4m3(float v) {
   return (uint8_t)__nv_cvt_float_to_fp8(v, __NV_SATFINITE, __NV_E4M3);
 }
 
+// Value of augmented column c (0..kAugCols-1) of a row with squared norm s:
+// database rows [n1 n2 n3 1 1 1], query rows [1 1 1 m1 m2 m3], where the three
+// BF16 terms sum to s (successive rounding of the remainders).
+__device__ __forceinline__ float aug_value(int aug, int c, float s) {
+  const float t1 = __bfloat162float(__float2bfloat16_rn(s));
+  const float r1 = s - t1;
+  const float t2 = __bfloat162float(__float2bfloat16_rn(r1));
+  const float t3 = r1 - t2;
+  const float terms[3] = {t1, t2, t3};
+  if (aug == kAugDatabase) return c < 3 ? terms[c] : 1.f;
+  return c < 3 ? 1.f : terms[c - 3];
+}
+
 __global__ void __launch_bounds__(kPrepWarps * 32) prep_rows_kernel(
     const float* __restrict__ x, long long ldx, int nrows, long long nrows_pad, int d, float* __restrict__ norms,
     float pad_norm, __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, long long ld16,
-    uint8_t* __restrict__ f8, float* __restrict__ scale, long long ld8, int vec4) {
+    uint8_t* __restrict__ f8, float* __restrict__ scale, long long ld8, int vec4, int aug) {
   const long long r = (long long)blockIdx.x * kPrepWarps + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (r >= nrows_pad) return;
@@ -76,6 +89,8 @@ __global__ void __launch_bounds__(kPrepWarps * 32) prep_rows_kernel(
   s = warp_sum(s);
   if (norms && lane == 0) norms[r] = s;
   if (!hi && !lo && !f8) return;
+  // query rows of the augmented forms are stored as -2q (exact in BF16)
+  const float hsc = aug == kAugQuery ? -2.f : 1.f;
   float inv = 1.f;
   if (f8) {
     m = warp_max(m);
@@ -91,17 +106,20 @@ __global__ void __launch_bounds__(kPrepWarps * 32) prep_rows_kernel(
         const __nv_bfloat16 h0 = __float2bfloat16_rn(v.x), h1 = __float2bfloat16_rn(v.y);
         const __nv_bfloat16 h2 = __float2bfloat16_rn(v.z), h3 = __float2bfloat16_rn(v.w);
         __nv_bfloat162 a, b;
-        a.x = h0; a.y = h1; b.x = h2; b.y = h3;
+        a.x = __float2bfloat16_rn(hsc * __bfloat162float(h0));
+        a.y = __float2bfloat16_rn(hsc * __bfloat162float(h1));
+        b.x = __float2bfloat16_rn(hsc * __bfloat162float(h2));
+        b.y = __float2bfloat16_rn(hsc * __bfloat162float(h3));
         uint2 pk;
         pk.x = *reinterpret_cast<uint32_t*>(&a);
         pk.y = *reinterpret_cast<uint32_t*>(&b);
         *reinterpret_cast<uint2*>(hi + r * ld16 + 4 * i) = pk;
         if (lo) {
           __nv_bfloat162 c, e;
-          c.x = __float2bfloat16_rn(v.x - __bfloat162float(h0));
-          c.y = __float2bfloat16_rn(v.y - __bfloat162float(h1));
-          e.x = __float2bfloat16_rn(v.z - __bfloat162float(h2));
-          e.y = __float2bfloat16_rn(v.w - __bfloat162float(h3));
+          c.x = __float2bfloat16_rn(hsc * (v.x - __bfloat162float(h0)));
+          c.y = __float2bfloat16_rn(hsc * (v.y - __bfloat162float(h1)));
+          e.x = __float2bfloat16_rn(hsc * (v.z - __bfloat162float(h2)));
+          e.y = __float2bfloat16_rn(hsc * (v.w - __bfloat162float(h3)));
           uint2 pl;
           pl.x = *reinterpret_cast<uint32_t*>(&c);
           pl.y = *reinterpret_cast<uint32_t*>(&e);
@@ -116,7 +134,8 @@ __global__ void __launch_bounds__(kPrepWarps * 32) prep_rows_kernel(
     }
     if (hi)
       for (long long i = d + lane; i < ld16; i += 32) {
-        hi[r * ld16 + i] = __float2bfloat16_rn(0.f);
+        const int c = (int)(i - d);
+        hi[r * ld16 + i] = __float2bfloat16_rn(aug && c < kAugCols ? aug_value(aug, c, s) : 0.f);
         if (lo) lo[r * ld16 + i] = __float2bfloat16_rn(0.f);
       }
     if (f8)
@@ -124,10 +143,16 @@ __global__ void __launch_bounds__(kPrepWarps * 32) prep_rows_kernel(
   } else {
     if (hi)
       for (long long i = lane; i < ld16; i += 32) {
-        const float v = i < d ? row[i] : 0.f;
-        const __nv_bfloat16 h = __float2bfloat16_rn(v);
-        hi[r * ld16 + i] = h;
-        if (lo) lo[r * ld16 + i] = __float2bfloat16_rn(v - __bfloat162float(h));
+        if (i < d) {
+          const float v = row[i];
+          const __nv_bfloat16 h = __float2bfloat16_rn(v);
+          hi[r * ld16 + i] = __float2bfloat16_rn(hsc * __bfloat162float(h));
+          if (lo) lo[r * ld16 + i] = __float2bfloat16_rn(hsc * (v - __bfloat162float(h)));
+        } else {
+          const int c = (int)(i - d);
+          hi[r * ld16 + i] = __float2bfloat16_rn(aug && c < kAugCols ? aug_value(aug, c, s) : 0.f);
+          if (lo) lo[r * ld16 + i] = __float2bfloat16_rn(0.f);
+        }
       }
     if (f8)
       for (long long i = lane; i < ld8; i += 32) {
@@ -175,12 +200,12 @@ __global__ void fill_results_kernel(int* idx, float* dist, long long n) {
 
 cudaError_t launch_prep_rows(const float* x, long long ldx, int nrows, long long nrows_pad, int d, float* norms,
                              float pad_norm, __nv_bfloat16* hi, __nv_bfloat16* lo, long long ld16, uint8_t* f8,
-                             float* scale, long long ld8, cudaStream_t st) {
+                             float* scale, long long ld8, cudaStream_t st, int aug) {
   if (nrows_pad <= 0) return cudaSuccess;
   const int vec4 = (d % 4 == 0) && (ldx % 4 == 0) && ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
   const long long blocks = (nrows_pad + kPrepWarps - 1) / kPrepWarps;
   prep_rows_kernel<<<(unsigned)blocks, kPrepWarps * 32, 0, st>>>(x, ldx, nrows, nrows_pad, d, norms, pad_norm, hi,
-                                                                 lo, ld16, f8, scale, ld8, vec4);
+                                                                 lo, ld16, f8, scale, ld8, vec4, aug);
   return cudaGetLastError();
 }
 

@@ -187,6 +187,14 @@ __device__ __forceinline__ uint64_t sw128_kmajor_desc(uint32_t saddr) {
          ((uint64_t)1u << 46) | ((uint64_t)2u << 61);
 }
 
+// Same for a K-major tile with the 32-byte swizzle (TMA CU_TENSOR_MAP_SWIZZLE_32B,
+// 32-byte rows, 8-row groups 256 B apart), layout code 6.  One descriptor covers
+// one K step of 16 BF16 elements.  The tile base must be 256-byte aligned.
+__device__ __forceinline__ uint64_t sw32_kmajor_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1u << 16) | ((uint64_t)(256u >> 4) << 32) |
+         ((uint64_t)1u << 46) | ((uint64_t)6u << 61);
+}
+
 // Instruction descriptor: dense, f32 accumulate, K-major A and B.
 //   bits 4-5 D format (1 = f32); 7-9 A format; 10-12 B format; 17-22 N >> 3; 24-28 M >> 4.
 // Formats: kind::f16 -> 0 f16, 1 bf16; kind::f8f6f4 -> 0 e4m3, 1 e5m2.
@@ -195,6 +203,13 @@ __host__ __device__ constexpr uint32_t make_idesc(uint32_t a_fmt, uint32_t b_fmt
 }
 
 // ---------------------------------------------------------------- misc
+// min(a, b, c) in one instruction (three-input min, sm_100).
+__device__ __forceinline__ float fmin3(float a, float b, float c) {
+  float r;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
 __device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t* p) {
