@@ -546,92 +546,92 @@ __global__ void __launch_bounds__(kNumThreads, 1)
           tmem_ld_32x32b_x64(tmem_base + lane_base + slot * kBN + g * kHalfN + h * 64, v);
           tmem_ld_wait();
           STAT_END(ttm, st_tmem);
+          const int col0 = colh + h * 64;
+          // coarse distances of the 64 columns (two independent 32-column halves)
+          float da[32], db[32];
+          if (Tr::kFolded) {
+            // the accumulator already is ||q||^2 + ||x||^2 - 2 q.x
 #pragma unroll
-          for (int cc = 0; cc < 2; ++cc) {
-            const int col0 = colh + h * 64 + cc * 32;
-            const uint32_t* vc = v + cc * 32;
-            // coarse distance per column; bit j of m marks a survivor
-            float dd[32];
-            if (Tr::kFolded) {
-              // the accumulator already is ||q||^2 + ||x||^2 - 2 q.x
-#pragma unroll
-              for (int j = 0; j < 32; ++j) dd[j] = __uint_as_float(vc[j]);
-            } else {
-              const float4* xn4 = reinterpret_cast<const float4*>(p.db_norms + col0);
-              const float4* sx4 = reinterpret_cast<const float4*>(p.db_scale + col0);
-#pragma unroll
-              for (int j4 = 0; j4 < 8; ++j4) {
-                const float4 xn = __ldg(xn4 + j4);
-                const float4 sx = __ldg(sx4 + j4);
-                dd[4 * j4 + 0] = fmaf(__uint_as_float(vc[4 * j4 + 0]) * sx.x, m2s, xn.x);
-                dd[4 * j4 + 1] = fmaf(__uint_as_float(vc[4 * j4 + 1]) * sx.y, m2s, xn.y);
-                dd[4 * j4 + 2] = fmaf(__uint_as_float(vc[4 * j4 + 2]) * sx.z, m2s, xn.z);
-                dd[4 * j4 + 3] = fmaf(__uint_as_float(vc[4 * j4 + 3]) * sx.w, m2s, xn.w);
-              }
+            for (int j = 0; j < 32; ++j) {
+              da[j] = __uint_as_float(v[j]);
+              db[j] = __uint_as_float(v[32 + j]);
             }
-            // quick reject: chunk minimum by a shallow three-input-min tree
-            float mn;
-            {
-              float t[11];
+          } else {
+            const float4* xn4 = reinterpret_cast<const float4*>(p.db_norms + col0);
+            const float4* sx4 = reinterpret_cast<const float4*>(p.db_scale + col0);
 #pragma unroll
-              for (int i = 0; i < 10; ++i) t[i] = fmin3(dd[3 * i], dd[3 * i + 1], dd[3 * i + 2]);
-              t[10] = fminf(dd[30], dd[31]);
-              const float u0 = fmin3(t[0], t[1], t[2]), u1 = fmin3(t[3], t[4], t[5]);
-              const float u2 = fmin3(t[6], t[7], t[8]), u3 = fminf(t[9], t[10]);
-              mn = fminf(fminf(u0, u1), fminf(u2, u3));
+            for (int j4 = 0; j4 < 16; ++j4) {
+              const float4 xn = __ldg(xn4 + j4);
+              const float4 sx = __ldg(sx4 + j4);
+              float* dst = j4 < 8 ? da : db;
+              const int o = (j4 & 7) * 4;
+              dst[o + 0] = fmaf(__uint_as_float(v[4 * j4 + 0]) * sx.x, m2s, xn.x);
+              dst[o + 1] = fmaf(__uint_as_float(v[4 * j4 + 1]) * sx.y, m2s, xn.y);
+              dst[o + 2] = fmaf(__uint_as_float(v[4 * j4 + 2]) * sx.z, m2s, xn.z);
+              dst[o + 3] = fmaf(__uint_as_float(v[4 * j4 + 3]) * sx.w, m2s, xn.w);
             }
-            const bool hit = valid && mn <= thr;
-            if (__any_sync(0xffffffffu, hit)) {
-              uint32_t m = 0;
-              if (hit) {
-                // survivor mask, OR-combined in four independent partial masks
-                uint32_t pm[4] = {0u, 0u, 0u, 0u};
+          }
+          // survivor masks, each OR-combined in four independent partial masks
+          uint32_t ma, mb;
+          {
+            uint32_t pa[4] = {0u, 0u, 0u, 0u}, pb[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
-                for (int j = 0; j < 32; ++j) pm[j & 3] |= (dd[j] <= thr ? 1u : 0u) << j;
-                m = (pm[0] | pm[1]) | (pm[2] | pm[3]);
-                // database rows beyond nb (padding of the last tile) never survive
-                if (col0 + 32 > p.nb) m &= col0 >= p.nb ? 0u : ((1u << (p.nb - col0)) - 1u);
-              }
-              if (__any_sync(0xffffffffu, m != 0)) {
-                STAT_INC(st_slow, 1);
+            for (int j = 0; j < 32; ++j) {
+              pa[j & 3] |= (da[j] <= thr ? 1u : 0u) << j;
+              pb[j & 3] |= (db[j] <= thr ? 1u : 0u) << j;
+            }
+            ma = (pa[0] | pa[1]) | (pa[2] | pa[3]);
+            mb = (pb[0] | pb[1]) | (pb[2] | pb[3]);
+          }
+          if (!valid) ma = mb = 0u;
+          // database rows beyond nb (padding of the last tile) never survive
+          if (col0 + 64 > p.nb) {
+            const int lim = p.nb - col0;
+            ma &= lim <= 0 ? 0u : (lim >= 32 ? ~0u : ((1u << lim) - 1u));
+            mb &= lim <= 32 ? 0u : (lim >= 64 ? ~0u : ((1u << (lim - 32)) - 1u));
+          }
+          if (__any_sync(0xffffffffu, (ma | mb) != 0u)) {
+            STAT_INC(st_slow, 1);
 #ifdef CURPLSH_FUSED_STATS
-                {
-                  int mx = __popc(m);
+            {
+              int mx = __popc(ma) + __popc(mb);
 #pragma unroll
-                  for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-                  STAT_INC(st_iters, mx);
-                }
+              for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+              STAT_INC(st_iters, mx);
+            }
 #endif
-                // A lane rarely has more than two survivors in 32 columns: fetch
-                // them from registers with a select tree (no local memory), and
-                // only stash the chunk when there are more.
-                if (m) {
-                  const int j1 = __ffs(m) - 1;
-                  m &= m - 1;
-                  const float v1 = select32(dd, j1);
-                  if (n < P) pool[n] = make_key(Tr::kFolded ? v1 : v1 + qn, (uint32_t)(col0 + j1));
-                  ++n;
-                  STAT_INC(st_surv, 1);
-                }
-                if (m) {
-                  const int j2 = __ffs(m) - 1;
-                  m &= m - 1;
-                  const float v2 = select32(dd, j2);
-                  if (n < P) pool[n] = make_key(Tr::kFolded ? v2 : v2 + qn, (uint32_t)(col0 + j2));
-                  ++n;
-                  STAT_INC(st_surv, 1);
-                }
-                if (__any_sync(0xffffffffu, m != 0)) {
-                  float stash[32];
+            // A lane rarely has more than one survivor per 32 columns: take the
+            // first of each half with a register select tree (no local memory),
+            // a second one the same way, and stash only for the rare rest.
+            auto take = [&](uint32_t& m, const float (&dv)[32], int c0) {
+              if (m) {
+                const int j = __ffs(m) - 1;
+                m &= m - 1;
+                const float x = select32(dv, j);
+                if (n < P) pool[n] = make_key(Tr::kFolded ? x : x + qn, (uint32_t)(c0 + j));
+                ++n;
+                STAT_INC(st_surv, 1);
+              }
+            };
+            take(ma, da, col0);
+            take(mb, db, col0 + 32);
+            if (__any_sync(0xffffffffu, (ma | mb) != 0u)) {
+              take(ma, da, col0);
+              take(mb, db, col0 + 32);
+              if (__any_sync(0xffffffffu, (ma | mb) != 0u)) {
+                float stash[64];
 #pragma unroll
-                  for (int j = 0; j < 32; ++j) stash[j] = dd[j];
-                  while (m) {
-                    const int j = __ffs(m) - 1;
-                    m &= m - 1;
-                    if (n < P) pool[n] = make_key(Tr::kFolded ? stash[j] : stash[j] + qn, (uint32_t)(col0 + j));
-                    ++n;
-                    STAT_INC(st_surv, 1);
-                  }
+                for (int j = 0; j < 32; ++j) {
+                  stash[j] = da[j];
+                  stash[32 + j] = db[j];
+                }
+                uint64_t mm = ((uint64_t)mb << 32) | ma;
+                while (mm) {
+                  const int j = __ffsll((long long)mm) - 1;
+                  mm &= mm - 1;
+                  if (n < P) pool[n] = make_key(Tr::kFolded ? stash[j] : stash[j] + qn, (uint32_t)(col0 + j));
+                  ++n;
+                  STAT_INC(st_surv, 1);
                 }
               }
             }
