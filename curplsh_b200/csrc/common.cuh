@@ -75,34 +75,46 @@ constexpr int kNumThreads = 320;  // warp 0 TMA producer, warp 1 MMA issuer, war
 constexpr int kAugCols = 6;
 constexpr int kEpiWarps = 8;
 
-struct FusedParams {
-  // problem
-  int nq;           // real number of queries
-  int nb;           // real number of database rows
-  int d;            // dimension
-  int kprime;       // candidates kept per query (before the FP32 rerank)
-  int pool_cap;     // capacity of one candidate pool (entries)
-  int form;         // Form
-  // schedule: flattened (query block, tile) space split evenly across CTAs
-  int num_qblocks;  // G
-  int num_tiles;    // T
-  long long work_per_cta;  // W
-  int units_per_block;     // U: max CTAs (units) that share one query block
-  // inputs
-  const float* db_norms;   // [nb_pad] squared norms, +inf for padding rows
+// One work item of the fused pass: a query batch against one resident
+// database.  A launch serves a list of items that share the form and the
+// dimension; the (item, query block, tile) space of all of them is flattened
+// and split evenly across the CTAs.  Items travel in the kernel parameters.
+struct FusedItem {
+  int nq;                  // real number of queries
+  int nb;                  // real number of database rows
+  int kprime;              // candidates kept per query (before the FP32 rerank)
+  int pool_cap;            // capacity of one candidate pool (entries)
+  int num_qblocks;         // G_i = ceil(nq / 128)
+  int num_tiles;           // T_i = ceil(nb / 256)
+  int units_per_block;     // U_i: max CTAs (units) that share one query block of this item
+  int pad0;
+  long long work_begin;    // flattened offset of this item's first (block, tile)
+  long long work_end;      // work_begin + G_i * T_i
+  const float* db_norms;   // [nb_pad] squared norms, +inf for padding rows (FP8 form)
   const float* db_scale;   // [nb_pad] fp8 per-vector scales (FP8 form)
   const float* q_norms;    // [nq_pad]
   const float* q_scale;    // [nq_pad] (FP8 form)
-  // outputs / scratch
-  uint64_t* pools;         // [G*128][U][2][pool_cap]
-  int* pool_counts;        // [G*128][U][2]
+  uint64_t* pools;         // [G_i*128][U_i][2][pool_cap]
+  int* pool_counts;        // [G_i*128][U_i][2]
   uint32_t* q_bound;       // [nq_pad] shared per-query bound (ordered bits), init kOrdInf
   uint32_t* q_bound_half;  // [nq_pad][2] per-query, per-half (k'/2)-th bounds, init kOrdInf
+};
+
+// Tensor maps of one item, in this order.
+enum FusedMap : int { kMapQHi = 0, kMapQLo, kMapXHi, kMapXLo, kMapQTail, kMapXTail, kMapsPerItem };
+
+struct FusedBatch {
+  int num_items;
+  int form;
+  int d;                   // dimension shared by every item of the launch
+  int pad0;
+  long long total_work;    // sum of G_i * T_i
+  long long work_per_cta;  // W
   uint32_t* status;        // device error word
   unsigned long long* stats;  // per-role cycle counters, written only by builds with CURPLSH_FUSED_STATS
 };
 
-// Counter slots of FusedParams::stats (instrumented builds).
+// Counter slots of FusedBatch::stats (instrumented builds).
 enum FusedStat : int {
   kStatProducerWaitEmpty = 0,  // producer lane: cycles waiting for a free stage
   kStatMmaWaitFull,            // MMA lane: cycles waiting for TMA data
@@ -118,19 +130,6 @@ enum FusedStat : int {
   kStatLoopIters,              // survivor-append loop iterations executed by warps
   kStatTmemCycles,             // epilogue warps (lane 0): cycles in TMEM loads + waits
   kStatCount
-};
-
-struct MergeParams {
-  int nq, nb, d, k, kprime, pool_cap, units_per_block;
-  const uint64_t* pools;
-  const int* pool_counts;
-  const float* queries;    // [nq x d] fp32
-  const float* db;         // [nb x d] fp32 (row stride ld_db)
-  long long ld_db;
-  const uint32_t* q_bound;
-  int* out_idx;            // [nq x k]
-  float* out_dist;         // [nq x k]
-  uint32_t* status;
 };
 
 }  // namespace curplsh_b200

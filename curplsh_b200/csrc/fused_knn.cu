@@ -144,23 +144,38 @@ __device__ __forceinline__ uint32_t stage_tail_off(const SmemLayout& L) {
 }
 
 // ------------------------------------------------------------------ schedule
+// Launch arguments: the batch header, then per-item scalars and tensor maps.
+template <int MAXI>
+struct FusedArgs {
+  FusedBatch B;
+  FusedItem items[MAXI];
+  CUtensorMap maps[MAXI * kMapsPerItem];
+};
+
 // Walks the contiguous range [cta*W, min(total,(cta+1)*W)) of the flattened
-// (query block, tile) space as units (query block, [t0, t1)).
+// (item, query block, tile) space as units (item, query block, [t0, t1)).
+// u_ord numbers the CTAs that share one query block (0 = the first CTA).
 struct UnitWalk {
   long long pos, end, W;
-  int T;
-  __device__ UnitWalk(int cta, long long W_, int G, int T_) : W(W_), T(T_) {
-    const long long total = (long long)G * T_;
-    pos = (long long)cta * W_;
-    end = pos + W_ < total ? pos + W_ : total;
+  int ii;
+  __device__ UnitWalk(int cta, const FusedBatch& B) : W(B.work_per_cta), ii(0) {
+    pos = (long long)cta * W;
+    end = pos + W < B.total_work ? pos + W : B.total_work;
   }
-  __device__ bool next(int cta, int& qb, int& t0, int& t1, int& u_ord) {
+  template <int MAXI>
+  __device__ bool next(int cta, const FusedArgs<MAXI>& A, int& item, int& qb, int& t0, int& t1, int& u_ord) {
     if (pos >= end) return false;
-    qb = (int)(pos / T);
-    t0 = (int)(pos - (long long)qb * T);
+    while (ii < A.B.num_items && A.items[ii].work_end <= pos) ++ii;
+    if (ii >= A.B.num_items) return false;
+    const long long wb = A.items[ii].work_begin;
+    const int T = A.items[ii].num_tiles;
+    const long long lp = pos - wb;
+    qb = (int)(lp / T);
+    t0 = (int)(lp - (long long)qb * T);
     const long long len = (end - pos) < (long long)(T - t0) ? (end - pos) : (long long)(T - t0);
     t1 = t0 + (int)len;
-    u_ord = cta - (int)(((long long)qb * T) / W);
+    u_ord = cta - (int)((wb + (long long)qb * T) / W);
+    item = ii;
     pos += len;
     return true;
   }
@@ -202,14 +217,14 @@ __device__ __forceinline__ float thr_from(float dstar, float qn) {
 }
 
 // Instrumentation (compiled in only with -DCURPLSH_FUSED_STATS): per-role
-// cycle counters accumulated in registers and added to p.stats at exit.
+// cycle counters accumulated in registers and added to B.stats at exit.
 #ifdef CURPLSH_FUSED_STATS
 #define STAT_DECL(name) unsigned long long name = 0
 #define STAT_BEGIN(t) const long long t = clock64()
 #define STAT_END(t, acc) acc += (unsigned long long)(clock64() - t)
 #define STAT_INC(acc, v) acc += (unsigned long long)(v)
 #define STAT_FLUSH(slot, acc) \
-  if (p.stats) atomicAdd(&p.stats[slot], acc)
+  if (B.stats) atomicAdd(&B.stats[slot], acc)
 #else
 #define STAT_DECL(name)
 #define STAT_BEGIN(t)
@@ -233,16 +248,13 @@ __device__ __forceinline__ float select32(const float (&v)[32], int j) {
 }
 
 // ------------------------------------------------------------------ kernel
-template <int FORM>
-__global__ void __launch_bounds__(kNumThreads, 1)
-    fused_knn_kernel(const __grid_constant__ CUtensorMap tm_q_hi, const __grid_constant__ CUtensorMap tm_q_lo,
-                     const __grid_constant__ CUtensorMap tm_x_hi, const __grid_constant__ CUtensorMap tm_x_lo,
-                     const __grid_constant__ CUtensorMap tm_q_tail, const __grid_constant__ CUtensorMap tm_x_tail,
-                     const FusedParams p) {
+template <int FORM, int MAXI>
+__global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_constant__ FusedArgs<MAXI> A) {
   using Tr = FormTraits<FORM>;
+  const FusedBatch& B = A.B;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const SmemLayout L = make_layout(FORM, p.d);
+  const SmemLayout L = make_layout(FORM, B.d);
   const int S = L.stages;
 
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.bar_off);
@@ -286,29 +298,30 @@ __global__ void __launch_bounds__(kNumThreads, 1)
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
 
-  const int G = p.num_qblocks;
-  const int T = p.num_tiles;
-  const long long W = p.work_per_cta;
   const int KC = Tr::kChunkElems;
+  auto maps_of = [&](int ii) { return &A.maps[ii * kMapsPerItem]; };
 
   if (warp == 0) {
     // ------------------------------------------------------------ producer
     if (lane == 0) {
-      tma_prefetch_desc(&tm_q_hi);
-      tma_prefetch_desc(&tm_x_hi);
-      if (Tr::kAParts > 1) tma_prefetch_desc(&tm_q_lo);
-      if (Tr::kBParts > 1) tma_prefetch_desc(&tm_x_lo);
       const uint64_t pol_db = l2_policy_evict_first();
       const uint64_t pol_q = l2_policy_evict_last();
-      UnitWalk walk(blockIdx.x, W, G, T);
-      int qb, t0, t1, u_ord, unit = 0;
+      UnitWalk walk(blockIdx.x, B);
+      int ii, qb, t0, t1, u_ord, unit = 0;
       uint32_t it = 0;
       bool ok = true;
       STAT_DECL(st_wait);
-      while (ok && walk.next(blockIdx.x, qb, t0, t1, u_ord)) {
+      while (ok && walk.next(blockIdx.x, A, ii, qb, t0, t1, u_ord)) {
+        const CUtensorMap* mp = maps_of(ii);
+        const CUtensorMap& tm_q_hi = mp[kMapQHi];
+        const CUtensorMap& tm_q_lo = mp[kMapQLo];
+        const CUtensorMap& tm_x_hi = mp[kMapXHi];
+        const CUtensorMap& tm_x_lo = mp[kMapXLo];
+        const CUtensorMap& tm_q_tail = mp[kMapQTail];
+        const CUtensorMap& tm_x_tail = mp[kMapXTail];
         if (!L.a_stream) {
           if (unit > 0 && !wait_or_abort(a_empty, (unit - 1) & 1, abort_flag)) {
-            raise_abort(abort_flag, p.status, kErrWaitTimeout);
+            raise_abort(abort_flag, B.status, kErrWaitTimeout);
             ok = false;
             break;
           }
@@ -328,7 +341,7 @@ __global__ void __launch_bounds__(kNumThreads, 1)
             const int s = (int)(it % (uint32_t)S);
             STAT_BEGIN(tw);
             if (!wait_or_abort(&empty[s], ((it / S) & 1u) ^ 1u, abort_flag)) {
-              raise_abort(abort_flag, p.status, kErrWaitTimeout);
+              raise_abort(abort_flag, B.status, kErrWaitTimeout);
               ok = false;
               break;
             }
@@ -360,16 +373,16 @@ __global__ void __launch_bounds__(kNumThreads, 1)
     if (lane == 0) {
       constexpr uint32_t fmt = Tr::kFP8 ? 0u : 1u;  // e4m3 : bf16
       constexpr uint32_t idesc = make_idesc(fmt, fmt, kBM, kBN);
-      UnitWalk walk(blockIdx.x, W, G, T);
-      int qb, t0, t1, u_ord, unit = 0;
+      UnitWalk walk(blockIdx.x, B);
+      int ii, qb, t0, t1, u_ord, unit = 0;
       uint32_t it = 0, tc = 0;
       bool ok = true;
       STAT_DECL(st_full);
       STAT_DECL(st_acc);
-      while (ok && walk.next(blockIdx.x, qb, t0, t1, u_ord)) {
+      while (ok && walk.next(blockIdx.x, A, ii, qb, t0, t1, u_ord)) {
         if (!L.a_stream) {
           if (!wait_or_abort(a_full, unit & 1, abort_flag)) {
-            raise_abort(abort_flag, p.status, kErrWaitTimeout);
+            raise_abort(abort_flag, B.status, kErrWaitTimeout);
             break;
           }
           tc_fence_after();
@@ -378,7 +391,7 @@ __global__ void __launch_bounds__(kNumThreads, 1)
           const uint32_t slot = tc & 1u, use = tc >> 1;
           STAT_BEGIN(ta);
           if (!wait_or_abort(&acc_empty[slot], (use & 1u) ^ 1u, abort_flag)) {
-            raise_abort(abort_flag, p.status, kErrWaitTimeout);
+            raise_abort(abort_flag, B.status, kErrWaitTimeout);
             ok = false;
             break;
           }
@@ -391,7 +404,7 @@ __global__ void __launch_bounds__(kNumThreads, 1)
             const int s = (int)(it % (uint32_t)S);
             STAT_BEGIN(tf);
             if (!wait_or_abort(&full[s], (it / S) & 1u, abort_flag)) {
-              raise_abort(abort_flag, p.status, kErrWaitTimeout);
+              raise_abort(abort_flag, B.status, kErrWaitTimeout);
               ok = false;
               break;
             }
@@ -444,10 +457,8 @@ __global__ void __launch_bounds__(kNumThreads, 1)
     const int row = lg * 32 + lane;
     uint32_t* hist = hist_all + ew * 256;
     const uint32_t lane_base = (uint32_t)(lg * 32) << 16;
-    const int P = p.pool_cap;
-    const int U = p.units_per_block;
-    UnitWalk walk(blockIdx.x, W, G, T);
-    int qb, t0, t1, u_ord;
+    UnitWalk walk(blockIdx.x, B);
+    int ii, qb, t0, t1, u_ord;
     uint32_t tc = 0;
     bool ok = true;
     STAT_DECL(st_wait);
@@ -459,11 +470,14 @@ __global__ void __launch_bounds__(kNumThreads, 1)
     STAT_DECL(st_iters);
     STAT_DECL(st_tmem);
 #ifdef CURPLSH_FUSED_STATS
-    if (threadIdx.x == 64 && p.stats) g_radix_pass_counter = &p.stats[kStatRadixPasses];
+    if (threadIdx.x == 64 && B.stats) g_radix_pass_counter = &B.stats[kStatRadixPasses];
 #endif
-    while (ok && walk.next(blockIdx.x, qb, t0, t1, u_ord)) {
+    while (ok && walk.next(blockIdx.x, A, ii, qb, t0, t1, u_ord)) {
+      const FusedItem& p = A.items[ii];
+      const int P = p.pool_cap;
+      const int U = p.units_per_block;
       if (u_ord < 0 || u_ord >= U) {
-        raise_abort(abort_flag, p.status, kErrBadSchedule);
+        raise_abort(abort_flag, B.status, kErrBadSchedule);
         break;
       }
       const int q = qb * kBM + row;
@@ -531,7 +545,7 @@ __global__ void __launch_bounds__(kNumThreads, 1)
         }
         STAT_BEGIN(tw);
         if (!wait_or_abort(&acc_full[slot], use & 1u, abort_flag)) {
-          raise_abort(abort_flag, p.status, kErrWaitTimeout);
+          raise_abort(abort_flag, B.status, kErrWaitTimeout);
           ok = false;
           break;
         }
@@ -641,7 +655,7 @@ __global__ void __launch_bounds__(kNumThreads, 1)
         __syncwarp();
         if (lane == 0) mbar_arrive(&acc_empty[slot]);
         STAT_END(tfl, st_filter);
-        if (n > P) atomicOr(p.status, kErrPoolOverflow);
+        if (n > P) atomicOr(B.status, kErrPoolOverflow);
         // a pool must have room for the next tile's half (kHalfN columns)
         refresh(__ballot_sync(0xffffffffu, n > P - kHalfN), p.kprime);
       }
@@ -670,7 +684,7 @@ __global__ void __launch_bounds__(kNumThreads, 1)
     tmem_dealloc(tmem_base, 512);
   }
 #ifdef CURPLSH_FUSED_STATS
-  if (threadIdx.x == 0 && p.stats) atomicAdd(&p.stats[kStatCtaCycles], (unsigned long long)(clock64() - t_kernel));
+  if (threadIdx.x == 0 && B.stats) atomicAdd(&B.stats[kStatCtaCycles], (unsigned long long)(clock64() - t_kernel));
 #endif
 }
 
@@ -712,98 +726,185 @@ bool make_map(CUtensorMap* m, const void* base, bool fp8, long long rows, long l
   return r == CUDA_SUCCESS;
 }
 
-template <int FORM>
-cudaError_t launch_form(const FusedLaunch& f, const FusedParams& p, int grid, uint32_t smem, cudaStream_t st) {
+template <int FORM, int MAXI>
+cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, int n, const FusedBatchPlan& bp,
+                        uint32_t* status, unsigned long long* stats, uint32_t smem, cudaStream_t st) {
   static bool attr_done[16] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr_done[dev & 15]) {
-    cudaError_t e = cudaFuncSetAttribute(fused_knn_kernel<FORM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(fused_knn_kernel<FORM, MAXI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          227 * 1024);
     if (e != cudaSuccess) return e;
     attr_done[dev & 15] = true;
   }
-  CUtensorMap mqh, mql, mxh, mxl, mqt, mxt;
+  FusedArgs<MAXI> a;
+  memset(&a, 0, sizeof(a));
+  a.B.num_items = n;
+  a.B.form = FORM;
+  a.B.d = specs[0].d;
+  a.B.total_work = bp.total_work;
+  a.B.work_per_cta = bp.work_per_cta;
+  a.B.status = status;
+  a.B.stats = stats;
   const bool fp8 = FORM == kFormFP8;
-  const void* qh = fp8 ? (const void*)f.q8 : (const void*)f.qh;
-  const void* xh = fp8 ? (const void*)f.x8 : (const void*)f.xh;
-  const long long ldq = fp8 ? f.ld8 : f.ld16;
-  if (!make_map(&mqh, qh, fp8, f.nq_pad, ldq, kBM) || !make_map(&mxh, xh, fp8, f.nb_pad, ldq, kBN))
-    return cudaErrorInvalidValue;
-  if (FORM == kFormExact) {
-    if (!make_map(&mql, f.ql, false, f.nq_pad, f.ld16, kBM) || !make_map(&mxl, f.xl, false, f.nb_pad, f.ld16, kBN))
+  for (int i = 0; i < n; ++i) {
+    const FusedItemSpec& f = specs[i];
+    const FusedItemPlan& pl = plans[i];
+    FusedItem& it = a.items[i];
+    it.nq = f.nq;
+    it.nb = f.nb;
+    it.kprime = f.kprime;
+    it.pool_cap = f.pool_cap;
+    it.num_qblocks = pl.num_qblocks;
+    it.num_tiles = pl.num_tiles;
+    it.units_per_block = pl.units_per_block;
+    it.work_begin = pl.work_begin;
+    it.work_end = pl.work_end;
+    it.db_norms = f.xn;
+    it.db_scale = f.xs;
+    it.q_norms = f.qn;
+    it.q_scale = f.qs;
+    it.pools = f.pools;
+    it.pool_counts = f.pool_counts;
+    it.q_bound = f.q_bound;
+    it.q_bound_half = f.q_bound_half;
+    CUtensorMap* m = &a.maps[i * kMapsPerItem];
+    const void* qh = fp8 ? (const void*)f.q8 : (const void*)f.qh;
+    const void* xh = fp8 ? (const void*)f.x8 : (const void*)f.xh;
+    const long long ldq = fp8 ? f.ld8 : f.ld16;
+    if (!make_map(&m[kMapQHi], qh, fp8, f.nq_pad, ldq, kBM) || !make_map(&m[kMapXHi], xh, fp8, f.nb_pad, ldq, kBN))
       return cudaErrorInvalidValue;
-  } else {
-    mql = mqh;
-    mxl = mxh;
+    if (FORM == kFormExact) {
+      if (!make_map(&m[kMapQLo], f.ql, false, f.nq_pad, f.ld16, kBM) ||
+          !make_map(&m[kMapXLo], f.xl, false, f.nb_pad, f.ld16, kBN))
+        return cudaErrorInvalidValue;
+    } else {
+      m[kMapQLo] = m[kMapQHi];
+      m[kMapXLo] = m[kMapXHi];
+    }
+    if (FORM != kFormFP8) {
+      if (!make_map(&m[kMapQTail], f.qh, false, f.nq_pad, f.ld16, kBM, true) ||
+          !make_map(&m[kMapXTail], f.xh, false, f.nb_pad, f.ld16, kBN, true))
+        return cudaErrorInvalidValue;
+    } else {
+      m[kMapQTail] = m[kMapQHi];
+      m[kMapXTail] = m[kMapXHi];
+    }
   }
-  if (FORM != kFormFP8) {
-    if (!make_map(&mqt, f.qh, false, f.nq_pad, f.ld16, kBM, true) ||
-        !make_map(&mxt, f.xh, false, f.nb_pad, f.ld16, kBN, true))
-      return cudaErrorInvalidValue;
-  } else {
-    mqt = mqh;
-    mxt = mxh;
-  }
-  fused_knn_kernel<FORM><<<grid, kNumThreads, smem, st>>>(mqh, mql, mxh, mxl, mqt, mxt, p);
+  fused_knn_kernel<FORM, MAXI><<<bp.grid, kNumThreads, smem, st>>>(a);
   return cudaGetLastError();
+}
+
+template <int FORM>
+cudaError_t launch_form_any(const FusedItemSpec* specs, const FusedItemPlan* plans, int n, const FusedBatchPlan& bp,
+                            uint32_t* status, unsigned long long* stats, uint32_t smem, cudaStream_t st) {
+  if (n == 1) return launch_form<FORM, 1>(specs, plans, n, bp, status, stats, smem, st);
+  return launch_form<FORM, kFusedMaxItems>(specs, plans, n, bp, status, stats, smem, st);
 }
 
 }  // namespace
 
-void plan_fused(int nq, int nb, int num_sms, FusedPlan* out) {
-  FusedPlan& pl = *out;
-  pl.num_qblocks = (nq + kBM - 1) / kBM;
-  pl.num_tiles = (nb + kBN - 1) / kBN;
-  const long long total = (long long)pl.num_qblocks * pl.num_tiles;
-  long long grid = num_sms < total ? num_sms : total;
-  if (grid < 1) grid = 1;
-  pl.work_per_cta = (total + grid - 1) / grid;
-  pl.grid = (int)((total + pl.work_per_cta - 1) / pl.work_per_cta);
-  int U = 1;
-  for (int qb = 0; qb < pl.num_qblocks; ++qb) {
-    const long long first = ((long long)qb * pl.num_tiles) / pl.work_per_cta;
-    const long long last = ((long long)(qb + 1) * pl.num_tiles - 1) / pl.work_per_cta;
-    if (last - first + 1 > U) U = (int)(last - first + 1);
+void plan_fused_batch(const FusedItemSpec* specs, int n, int max_ctas, FusedItemPlan* plans, FusedBatchPlan* out) {
+  long long total = 0;
+  for (int i = 0; i < n; ++i) {
+    FusedItemPlan& pl = plans[i];
+    pl.num_qblocks = specs[i].nb > 0 ? (specs[i].nq + kBM - 1) / kBM : 0;
+    pl.num_tiles = (specs[i].nb + kBN - 1) / kBN;
+    pl.work_begin = total;
+    total += (long long)pl.num_qblocks * pl.num_tiles;
+    pl.work_end = total;
   }
-  pl.units_per_block = U;
+  long long grid = max_ctas < total ? max_ctas : total;
+  if (grid < 1) grid = 1;
+  out->total_work = total;
+  out->work_per_cta = total > 0 ? (total + grid - 1) / grid : 1;
+  out->grid = total > 0 ? (int)((total + out->work_per_cta - 1) / out->work_per_cta) : 0;
+  const long long W = out->work_per_cta;
+  for (int i = 0; i < n; ++i) {
+    FusedItemPlan& pl = plans[i];
+    int U = 1;
+    for (int qb = 0; qb < pl.num_qblocks; ++qb) {
+      const long long first = (pl.work_begin + (long long)qb * pl.num_tiles) / W;
+      const long long last = (pl.work_begin + (long long)(qb + 1) * pl.num_tiles - 1) / W;
+      if (last - first + 1 > U) U = (int)(last - first + 1);
+    }
+    pl.units_per_block = U;
+  }
+}
+
+void plan_fused(int nq, int nb, int num_sms, FusedPlan* out) {
+  FusedItemSpec s{};
+  s.nq = nq;
+  s.nb = nb;
+  FusedItemPlan ip;
+  FusedBatchPlan bp;
+  plan_fused_batch(&s, 1, num_sms, &ip, &bp);
+  out->num_qblocks = ip.num_qblocks;
+  out->num_tiles = ip.num_tiles;
+  out->work_per_cta = bp.work_per_cta;
+  out->grid = bp.grid;
+  out->units_per_block = ip.units_per_block;
 }
 
 uint32_t fused_smem_bytes(int form, int d) { return make_layout(form, d).total; }
 
-cudaError_t launch_fused(const FusedLaunch& f, cudaStream_t st) {
-  FusedParams p{};
-  p.nq = f.nq;
-  p.nb = f.nb;
-  p.d = f.d;
-  p.kprime = f.kprime;
-  p.pool_cap = f.pool_cap;
-  p.form = f.form;
-  p.num_qblocks = f.plan.num_qblocks;
-  p.num_tiles = f.plan.num_tiles;
-  p.work_per_cta = f.plan.work_per_cta;
-  p.units_per_block = f.plan.units_per_block;
-  p.db_norms = f.xn;
-  p.db_scale = f.xs;
-  p.q_norms = f.qn;
-  p.q_scale = f.qs;
-  p.pools = f.pools;
-  p.pool_counts = f.pool_counts;
-  p.q_bound = f.q_bound;
-  p.q_bound_half = f.q_bound_half;
-  p.status = f.status;
-  p.stats = f.stats;
-  const uint32_t smem = make_layout(f.form, f.d).total;
-  switch (f.form) {
+cudaError_t launch_fused_batch(int form, const FusedItemSpec* specs, const FusedItemPlan* plans, int n,
+                               const FusedBatchPlan& bp, uint32_t* status, unsigned long long* stats,
+                               cudaStream_t st) {
+  if (n < 1 || n > kFusedMaxItems) return cudaErrorInvalidValue;
+  for (int i = 1; i < n; ++i)
+    if (specs[i].d != specs[0].d) return cudaErrorInvalidValue;
+  if (bp.grid == 0) return cudaSuccess;
+  const uint32_t smem = make_layout(form, specs[0].d).total;
+  switch (form) {
     case kFormExact:
-      return launch_form<kFormExact>(f, p, f.plan.grid, smem, st);
+      return launch_form_any<kFormExact>(specs, plans, n, bp, status, stats, smem, st);
     case kFormBF16:
-      return launch_form<kFormBF16>(f, p, f.plan.grid, smem, st);
+      return launch_form_any<kFormBF16>(specs, plans, n, bp, status, stats, smem, st);
     case kFormFP8:
-      return launch_form<kFormFP8>(f, p, f.plan.grid, smem, st);
+      return launch_form_any<kFormFP8>(specs, plans, n, bp, status, stats, smem, st);
     default:
       return cudaErrorInvalidValue;
   }
+}
+
+cudaError_t launch_fused(const FusedLaunch& f, cudaStream_t st) {
+  FusedItemSpec s{};
+  s.nq = f.nq;
+  s.nb = f.nb;
+  s.d = f.d;
+  s.kprime = f.kprime;
+  s.pool_cap = f.pool_cap;
+  s.nq_pad = f.nq_pad;
+  s.nb_pad = f.nb_pad;
+  s.ld16 = f.ld16;
+  s.ld8 = f.ld8;
+  s.qh = f.qh;
+  s.ql = f.ql;
+  s.q8 = f.q8;
+  s.qn = f.qn;
+  s.qs = f.qs;
+  s.xh = f.xh;
+  s.xl = f.xl;
+  s.x8 = f.x8;
+  s.xn = f.xn;
+  s.xs = f.xs;
+  s.pools = f.pools;
+  s.pool_counts = f.pool_counts;
+  s.q_bound = f.q_bound;
+  s.q_bound_half = f.q_bound_half;
+  FusedItemPlan ip;
+  ip.num_qblocks = f.plan.num_qblocks;
+  ip.num_tiles = f.plan.num_tiles;
+  ip.units_per_block = f.plan.units_per_block;
+  ip.work_begin = 0;
+  ip.work_end = (long long)f.plan.num_qblocks * f.plan.num_tiles;
+  FusedBatchPlan bp;
+  bp.total_work = ip.work_end;
+  bp.work_per_cta = f.plan.work_per_cta;
+  bp.grid = f.plan.grid;
+  return launch_fused_batch(f.form, &s, &ip, 1, bp, f.status, f.stats, st);
 }
 
 }  // namespace curplsh_b200

@@ -44,6 +44,47 @@ void plan_fused(int nq, int nb, int num_sms, FusedPlan* out);
 uint32_t fused_smem_bytes(int form, int d);
 cudaError_t launch_fused(const FusedLaunch& f, cudaStream_t st);
 
+// ---- batched form: several (queries, database) items of one form and one
+// dimension in a single persistent launch.  The flattened work space is the
+// concatenation of every item's (query block, tile) grid; each CTA takes a
+// contiguous range of W units, so the load is balanced across items of any
+// size.  A single search is the one-item case.
+constexpr int kFusedMaxItems = 16;
+
+struct FusedItemSpec {
+  int nq, nb, d, kprime, pool_cap;
+  long long nq_pad, nb_pad, ld16, ld8;
+  const __nv_bfloat16* qh;
+  const __nv_bfloat16* ql;
+  const uint8_t* q8;
+  const float* qn;
+  const float* qs;
+  const __nv_bfloat16* xh;
+  const __nv_bfloat16* xl;
+  const uint8_t* x8;
+  const float* xn;
+  const float* xs;
+  uint64_t* pools;          // [G*128][U][2][pool_cap]
+  int* pool_counts;         // [G*128][U][2]
+  uint32_t* q_bound;        // [nq_pad], initialised to all ones
+  uint32_t* q_bound_half;   // [nq_pad][2], initialised to all ones
+};
+struct FusedItemPlan {
+  int num_qblocks, num_tiles, units_per_block;
+  long long work_begin, work_end;
+};
+struct FusedBatchPlan {
+  long long total_work = 0, work_per_cta = 1;
+  int grid = 0;
+};
+// Plans `n` items over at most `max_ctas` CTAs.  Only nq and nb of the specs
+// are read, so pool sizes (which depend on units_per_block) can be computed
+// from the plan before the pools are carved.
+void plan_fused_batch(const FusedItemSpec* specs, int n, int max_ctas, FusedItemPlan* plans, FusedBatchPlan* out);
+cudaError_t launch_fused_batch(int form, const FusedItemSpec* specs, const FusedItemPlan* plans, int n,
+                               const FusedBatchPlan& bp, uint32_t* status, unsigned long long* stats,
+                               cudaStream_t st);
+
 // Row preparation: squared norms (FP32), BF16 hi/lo split, FP8-E4M3 with a
 // per-row FP32 scale.  Rows in [nrows, nrows_pad) are written as zeros with
 // norm `pad_norm`.  Any of the output pointers may be null.  `aug` selects the
@@ -54,6 +95,24 @@ enum AugMode : int { kAugNone = 0, kAugDatabase = 1, kAugQuery = 2 };
 cudaError_t launch_prep_rows(const float* x, long long ldx, int nrows, long long nrows_pad, int d, float* norms,
                              float pad_norm, __nv_bfloat16* hi, __nv_bfloat16* lo, long long ld16, uint8_t* f8,
                              float* scale, long long ld8, cudaStream_t st, int aug = kAugNone);
+
+// The same preparation for several row ranges of one dimension in a single
+// launch.  Every pointer points at the segment's first row; source rows have
+// stride d; rows [nrows, rows) are written as padding.
+constexpr int kPrepMaxSegments = 128;
+struct PrepSegment {
+  const float* x;
+  int nrows;              // real rows
+  int rows;               // rows written (real + padding)
+  long long block_begin;  // filled by launch_prep_segments
+  float* norms;
+  __nv_bfloat16* hi;
+  __nv_bfloat16* lo;
+  uint8_t* f8;
+  float* scale;
+};
+cudaError_t launch_prep_segments(PrepSegment* segs, int n, int d, long long ld16, long long ld8, float pad_norm,
+                                 int aug, cudaStream_t st);
 
 // Plain squared (or not) L2 norms, as computeL2Norm.
 cudaError_t launch_l2_norms(const float* x, long long n, int d, float* norms, int squared, cudaStream_t st);
@@ -71,6 +130,28 @@ struct MergeLaunch {
   uint32_t* status;
 };
 cudaError_t launch_merge_rerank(const MergeLaunch& m, cudaStream_t st);
+
+// Batched merge: one CTA per query of every item; items share d.  An item is
+// a run of `nq` consecutive pool rows [row0, row0 + nq) of one fused item, so
+// several query batches that were concatenated into one fused item each keep
+// their own query and output pointers and their own k.
+constexpr int kMergeMaxItems = 128;
+struct MergeItem {
+  int nq, k, kprime, pool_cap, num_tiles, units_per_block;
+  int row0;                // first pool row of this item within its fused item
+  int pad0;
+  long long work_begin;    // the fused item's offset in its launch's flattened work space
+  long long work_per_cta;  // W of that launch
+  long long q_begin;       // first CTA of this item (filled by launch_merge_batch)
+  const uint64_t* pools;   // the fused item's pools and counts
+  const int* pool_counts;
+  const float* queries;    // [nq x d] fp32, row stride d
+  const float* db;         // database rows fp32, row stride ld_db
+  long long ld_db;
+  int* out_idx;            // [nq x k]
+  float* out_dist;
+};
+cudaError_t launch_merge_batch(MergeItem* items, int n, int d, uint32_t* status, cudaStream_t st);
 
 // Fill [n] ints / floats (N == 0 results, padding).
 cudaError_t launch_fill_results(int* idx, float* dist, long long n, cudaStream_t st);

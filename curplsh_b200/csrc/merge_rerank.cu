@@ -14,6 +14,8 @@
 //   3. bitonic sort by (exact distance, row) -- lower row first on ties -- and
 //      write the first k; missing results are (-1, FLT_MAX) as in
 //      src/internal/search.cu:94-101.
+#include <cstring>
+
 #include "common.cuh"
 #include "fused_knn.h"
 
@@ -39,33 +41,47 @@ __device__ __forceinline__ uint32_t block_incl_scan(uint32_t v, uint32_t* warp_t
 }
 
 struct MergeArgs {
-  MergeLaunch m;
-  long long W;
-  int T, U;
-  int kp2;  // power of two >= kprime
+  MergeItem items[kMergeMaxItems];
+  int num_items, d;
+  int kp2;     // power of two >= the largest kprime
+  int lcnt_n;  // room for the largest 2 * units_per_block, rounded to 4
+  uint32_t* status;
 };
 
-__global__ void __launch_bounds__(kMergeThreads) merge_rerank_kernel(const MergeArgs a) {
-  const MergeLaunch& m = a.m;
-  const int q = blockIdx.x;
+__global__ void __launch_bounds__(kMergeThreads) merge_rerank_kernel(const __grid_constant__ MergeArgs a) {
+  int lo = 0, hi = a.num_items - 1;  // last item with q_begin <= blockIdx.x
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (a.items[mid].q_begin <= (long long)blockIdx.x)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const int ii = lo;
+  const MergeItem& m = a.items[ii];
+  const int q = (int)((long long)blockIdx.x - m.q_begin);
   if (q >= m.nq) return;
+  const int d = a.d;
   extern __shared__ __align__(16) uint8_t sm[];
   uint64_t* cand = reinterpret_cast<uint64_t*>(sm);                       // [kp2]
   uint32_t* hist = reinterpret_cast<uint32_t*>(cand + a.kp2);             // [256]
   uint32_t* warp_tot = hist + 256;                                         // [8]
   uint32_t* misc = warp_tot + 8;                                           // [8]
-  int* lcnt = reinterpret_cast<int*>(misc + 8);                            // [2U]
-  float* qv = reinterpret_cast<float*>(lcnt + ((2 * a.U + 3) & ~3));      // [d]
+  int* lcnt = reinterpret_cast<int*>(misc + 8);                            // [lcnt_n]
+  float* qv = reinterpret_cast<float*>(lcnt + a.lcnt_n);                   // [d]
 
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
-  const int qb = q / kBM, row = q % kBM;
-  const long long first = ((long long)qb * a.T) / a.W;
-  const long long last = ((long long)(qb + 1) * a.T - 1) / a.W;
-  const int nlists = 2 * (int)(last - first + 1);
-  const size_t list0 = ((size_t)qb * kBM + row) * a.U * 2;  // pool-list index of (u=0, h=0)
+  const int prow = m.row0 + q;  // pool row within the fused item
+  const int qb = prow / kBM, row = prow % kBM;
+  const int T = m.num_tiles, U = m.units_per_block;
+  const long long W = m.work_per_cta;
+  const long long first = (m.work_begin + (long long)qb * T) / W;
+  const long long last = (m.work_begin + (long long)(qb + 1) * T - 1) / W;
+  const int nlists = T > 0 ? 2 * (int)(last - first + 1) : 0;  // an empty database has no pools
+  const size_t list0 = ((size_t)qb * kBM + row) * U * 2;  // pool-list index of (u=0, h=0)
 
-  for (int i = tid; i < m.d; i += kMergeThreads) qv[i] = m.queries[(size_t)q * m.d + i];
+  for (int i = tid; i < d; i += kMergeThreads) qv[i] = m.queries[(size_t)q * d + i];
   if (tid == 0) misc[0] = 0;
   for (int l = tid; l < nlists; l += kMergeThreads) lcnt[l] = m.pool_counts[list0 + l];
   __syncthreads();
@@ -125,7 +141,7 @@ __global__ void __launch_bounds__(kMergeThreads) merge_rerank_kernel(const Merge
   __syncthreads();
   int kept = (int)misc[0];
   if (kept > a.kp2) {
-    if (tid == 0) atomicOr(m.status, kErrPoolOverflow);
+    if (tid == 0) atomicOr(a.status, kErrPoolOverflow);
     kept = a.kp2;
   }
   // ---- 2. exact FP32 rerank, one warp per candidate
@@ -133,7 +149,7 @@ __global__ void __launch_bounds__(kMergeThreads) merge_rerank_kernel(const Merge
     const uint32_t idx = (uint32_t)(cand[c] & 0xFFFFFFFFu);
     const float* xr = m.db + (size_t)idx * m.ld_db;
     float s = 0.f;
-    for (int i = lane; i < m.d; i += 32) {
+    for (int i = lane; i < d; i += 32) {
       const float t = qv[i] - __ldg(xr + i);
       s = fmaf(t, t, s);
     }
@@ -176,17 +192,28 @@ __global__ void __launch_bounds__(kMergeThreads) merge_rerank_kernel(const Merge
 
 }  // namespace
 
-cudaError_t launch_merge_rerank(const MergeLaunch& m, cudaStream_t st) {
-  if (m.nq <= 0) return cudaSuccess;
-  MergeArgs a{};
-  a.m = m;
-  a.W = m.plan.work_per_cta;
-  a.T = m.plan.num_tiles;
-  a.U = m.plan.units_per_block;
+cudaError_t launch_merge_batch(MergeItem* items, int n, int d, uint32_t* status, cudaStream_t st) {
+  if (n < 1 || n > kMergeMaxItems) return cudaErrorInvalidValue;
+  MergeArgs a;
+  memset(&a, 0, sizeof(a));
+  long long qsum = 0;
+  int kpmax = 1, umax = 1;
+  for (int i = 0; i < n; ++i) {
+    items[i].q_begin = qsum;
+    qsum += items[i].nq > 0 ? items[i].nq : 0;
+    if (items[i].kprime > kpmax) kpmax = items[i].kprime;
+    if (items[i].units_per_block > umax) umax = items[i].units_per_block;
+    a.items[i] = items[i];
+  }
+  if (qsum == 0) return cudaSuccess;
+  a.num_items = n;
+  a.d = d;
+  a.status = status;
   int kp2 = 1;
-  while (kp2 < m.kprime) kp2 <<= 1;
+  while (kp2 < kpmax) kp2 <<= 1;
   a.kp2 = kp2;
-  const size_t smem = (size_t)kp2 * 8 + (256 + 8 + 8) * 4 + (size_t)((2 * a.U + 3) & ~3) * 4 + (size_t)m.d * 4 + 16;
+  a.lcnt_n = (2 * umax + 3) & ~3;
+  const size_t smem = (size_t)kp2 * 8 + (256 + 8 + 8) * 4 + (size_t)a.lcnt_n * 4 + (size_t)d * 4 + 16;
   static bool attr_done[16] = {};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -196,9 +223,31 @@ cudaError_t launch_merge_rerank(const MergeLaunch& m, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     attr_done[dev & 15] = true;
   }
-  if (smem > 200 * 1024) return cudaErrorInvalidValue;
-  merge_rerank_kernel<<<m.nq, kMergeThreads, smem, st>>>(a);
+  if (smem > 200 * 1024 || qsum > 0x7fffffffLL) return cudaErrorInvalidValue;
+  merge_rerank_kernel<<<(unsigned)qsum, kMergeThreads, smem, st>>>(a);
   return cudaGetLastError();
+}
+
+cudaError_t launch_merge_rerank(const MergeLaunch& m, cudaStream_t st) {
+  if (m.nq <= 0) return cudaSuccess;
+  MergeItem it{};
+  it.nq = m.nq;
+  it.k = m.k;
+  it.kprime = m.kprime;
+  it.pool_cap = m.pool_cap;
+  it.num_tiles = m.plan.num_tiles;
+  it.units_per_block = m.plan.units_per_block;
+  it.row0 = 0;
+  it.work_begin = 0;
+  it.work_per_cta = m.plan.work_per_cta;
+  it.pools = m.pools;
+  it.pool_counts = m.pool_counts;
+  it.queries = m.queries;
+  it.db = m.db;
+  it.ld_db = m.ld_db;
+  it.out_idx = m.out_idx;
+  it.out_dist = m.out_dist;
+  return launch_merge_batch(&it, 1, m.d, m.status, st);
 }
 
 }  // namespace curplsh_b200

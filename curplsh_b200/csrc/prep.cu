@@ -11,6 +11,8 @@
 // is handled without partial-warp shuffles or out-of-bounds rows.
 #include <cuda_fp8.h>
 
+#include <cstring>
+
 #include "common.cuh"
 #include "fused_knn.h"
 
@@ -49,13 +51,12 @@ __device__ __forceinline__ float aug_value(int aug, int c, float s) {
   return c < 3 ? 1.f : terms[c - 3];
 }
 
-__global__ void __launch_bounds__(kPrepWarps * 32) prep_rows_kernel(
-    const float* __restrict__ x, long long ldx, int nrows, long long nrows_pad, int d, float* __restrict__ norms,
-    float pad_norm, __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, long long ld16,
-    uint8_t* __restrict__ f8, float* __restrict__ scale, long long ld8, int vec4, int aug) {
-  const long long r = (long long)blockIdx.x * kPrepWarps + (threadIdx.x >> 5);
+// One warp prepares row r (< the padded row count) of one matrix.
+__device__ __forceinline__ void prep_row(const float* __restrict__ x, long long ldx, long long r, int nrows, int d,
+                                         float* __restrict__ norms, float pad_norm, __nv_bfloat16* __restrict__ hi,
+                                         __nv_bfloat16* __restrict__ lo, long long ld16, uint8_t* __restrict__ f8,
+                                         float* __restrict__ scale, long long ld8, int vec4, int aug) {
   const int lane = threadIdx.x & 31;
-  if (r >= nrows_pad) return;
   if (r >= nrows) {
     if (norms && lane == 0) norms[r] = pad_norm;
     if (scale && lane == 0) scale[r] = 0.f;
@@ -162,6 +163,41 @@ __global__ void __launch_bounds__(kPrepWarps * 32) prep_rows_kernel(
   }
 }
 
+__global__ void __launch_bounds__(kPrepWarps * 32) prep_rows_kernel(
+    const float* __restrict__ x, long long ldx, int nrows, long long nrows_pad, int d, float* __restrict__ norms,
+    float pad_norm, __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, long long ld16,
+    uint8_t* __restrict__ f8, float* __restrict__ scale, long long ld8, int vec4, int aug) {
+  const long long r = (long long)blockIdx.x * kPrepWarps + (threadIdx.x >> 5);
+  if (r >= nrows_pad) return;
+  prep_row(x, ldx, r, nrows, d, norms, pad_norm, hi, lo, ld16, f8, scale, ld8, vec4, aug);
+}
+
+struct PrepSegmentArgs {
+  PrepSegment seg[kPrepMaxSegments];
+  int vec4[kPrepMaxSegments];
+  int num, d, aug;
+  float pad_norm;
+  long long ld16, ld8;
+};
+
+// Several matrices (segments) of one dimension in one launch; each CTA
+// prepares kPrepWarps consecutive rows of one segment.
+__global__ void __launch_bounds__(kPrepWarps * 32) prep_segments_kernel(const __grid_constant__ PrepSegmentArgs a) {
+  int lo_i = 0, hi_i = a.num - 1;  // last segment with block_begin <= blockIdx.x
+  while (lo_i < hi_i) {
+    const int mid = (lo_i + hi_i + 1) >> 1;
+    if (a.seg[mid].block_begin <= (long long)blockIdx.x)
+      lo_i = mid;
+    else
+      hi_i = mid - 1;
+  }
+  const PrepSegment& g = a.seg[lo_i];
+  const long long r = ((long long)blockIdx.x - g.block_begin) * kPrepWarps + (threadIdx.x >> 5);
+  if (r >= g.rows) return;
+  prep_row(g.x, a.d, r, g.nrows, a.d, g.norms, a.pad_norm, g.hi, g.lo, a.ld16, g.f8, g.scale, a.ld8, a.vec4[lo_i],
+           a.aug);
+}
+
 __global__ void __launch_bounds__(kPrepWarps * 32)
     l2_norms_kernel(const float* __restrict__ x, long long n, int d, float* __restrict__ norms, int squared,
                     int vec4) {
@@ -206,6 +242,30 @@ cudaError_t launch_prep_rows(const float* x, long long ldx, int nrows, long long
   const long long blocks = (nrows_pad + kPrepWarps - 1) / kPrepWarps;
   prep_rows_kernel<<<(unsigned)blocks, kPrepWarps * 32, 0, st>>>(x, ldx, nrows, nrows_pad, d, norms, pad_norm, hi,
                                                                  lo, ld16, f8, scale, ld8, vec4, aug);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_prep_segments(PrepSegment* segs, int n, int d, long long ld16, long long ld8, float pad_norm,
+                                 int aug, cudaStream_t st) {
+  if (n < 1 || n > kPrepMaxSegments) return cudaErrorInvalidValue;
+  PrepSegmentArgs a;
+  memset(&a, 0, sizeof(a));
+  long long blocks = 0;
+  for (int i = 0; i < n; ++i) {
+    segs[i].block_begin = blocks;
+    blocks += (segs[i].rows + kPrepWarps - 1) / kPrepWarps;
+    a.seg[i] = segs[i];
+    a.vec4[i] = (d % 4 == 0) && ((reinterpret_cast<uintptr_t>(segs[i].x) & 15) == 0);
+  }
+  if (blocks == 0) return cudaSuccess;
+  if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
+  a.num = n;
+  a.d = d;
+  a.aug = aug;
+  a.pad_norm = pad_norm;
+  a.ld16 = ld16;
+  a.ld8 = ld8;
+  prep_segments_kernel<<<(unsigned)blocks, kPrepWarps * 32, 0, st>>>(a);
   return cudaGetLastError();
 }
 
