@@ -191,6 +191,138 @@ def run_reference(args, world, rank):
     return 0
 
 
+def run_batched(args, world, rank, local):
+    """--workload batched_uneven: 64 query batches of log-uniform size 1-4096
+    over 8 resident databases (N log-uniform 10k-2M, d in {64,128,256,512},
+    k in {1,10,100,1024}, N(0,1) data rounded to BF16), one step = one replay
+    of the captured batch graph.  Compared with the same items searched one by
+    one (search_ex in a loop on one stream)."""
+    import numpy as np
+    import torch
+
+    import curplsh_b200 as cb
+    import oracle
+    from curplsh_b200 import synth
+
+    torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
+    dbs_spec, batches = synth.batched_uneven_spec()
+    res = cb.DeviceResources(local)
+    stream = torch.cuda.Stream(device=dev)
+    precision = args.batch_form
+    dbs = []
+    for i, (n, d) in enumerate(dbs_spec):
+        x = synth.normal_bf16(n, d, seed=100 + i, device=dev)
+        ix = cb.IndexBF(res, d, cb.IndexBFConfig(device=local, precision=precision))
+        ix.add(n, x)
+        dbs.append((ix, x))
+    items = []
+    for j, (db, nq, k) in enumerate(batches):
+        ix, x = dbs[db]
+        q = synth.normal_bf16(nq, x.shape[1], seed=1000 + j + 7919 * rank, device=dev)
+        items.append((ix, q, k, torch.empty((nq, k), dtype=torch.int32, device=dev),
+                      torch.empty((nq, k), dtype=torch.float32, device=dev)))
+    total_q = sum(it[1].shape[0] for it in items)
+    flops = sum(2.0 * it[1].shape[0] * dbs[b[0]][1].shape[0] * it[1].shape[1] for it, b in zip(items, batches))
+    batch = cb.SearchBatch(items, precision=precision)
+    kernels, ws_bytes = batch.info()
+    # correctness: every item equals its search alone; a query sample against the oracle
+    batch.run(stream=stream)
+    mismatches = 0
+    recall_min, err_max = 1.0, 0.0
+    for j, (ix, q, k, oi, od) in enumerate(items):
+        ai = torch.empty_like(oi)
+        ad = torch.empty_like(od)
+        ix.search_ex(q.shape[0], q, k, ai, ad, precision, stream=stream)
+        stream.synchronize()
+        if not (torch.equal(ai, oi) and torch.equal(ad, od)):
+            mismatches += 1
+        if rank == 0 and not args.no_recall and j % 8 == 0:
+            x = dbs[batches[j][0]][1]
+            qs = q[:4].cpu().numpy()
+            rd, ri = oracle.knn(x.cpu().numpy(), qs, k)
+            rec, _ = oracle.recall_at_k(x.cpu().numpy(), qs, oi[:4].cpu().numpy(), rd)
+            gd = od[:4].cpu().numpy().astype(np.float64)
+            ok = ri >= 0
+            err = float(np.max(np.abs(gd[ok] - rd[ok]) / np.maximum(np.abs(rd[ok]), 1e-30))) if ok.any() else 0.0
+            recall_min = min(recall_min, rec)
+            err_max = max(err_max, err)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        stream.synchronize()
+        barrier(world)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+
+    sampler = ClockSampler(local)
+    sampler.__enter__()
+    ms_graph = timed(lambda: batch.run(stream=stream, wait=False))
+    sampler.__exit__(None, None, None)
+
+    def one_by_one():
+        for ix, q, k, oi, od in items:
+            ix.search_ex(q.shape[0], q, k, oi, od, precision, stream=stream)
+    ms_loop = timed(one_by_one)
+    # end to end: pinned host queries in, host results out, around the graph replay
+    qh = [torch.empty(tuple(it[1].shape), dtype=torch.float32, pin_memory=True).copy_(it[1].cpu()) for it in items]
+    ih = [torch.empty(tuple(it[3].shape), dtype=torch.int32, pin_memory=True) for it in items]
+    dh = [torch.empty(tuple(it[4].shape), dtype=torch.float32, pin_memory=True) for it in items]
+
+    def e2e_step():
+        with torch.cuda.stream(stream):
+            for it, h in zip(items, qh):
+                it[1].copy_(h, non_blocking=True)
+            batch.run(stream=stream, wait=False)
+            for it, a, b in zip(items, ih, dh):
+                a.copy_(it[3], non_blocking=True)
+                b.copy_(it[4], non_blocking=True)
+    ms_e2e = timed(e2e_step)
+    if rank == 0:
+        hbm, bf16_burst, bf16_sust, peak_kind = load_peaks()
+        p_form = bf16_burst / 3.0 if precision == 0 else (2 * bf16_burst if precision == 2 else bf16_burst)
+        achieved = flops / (ms_graph / 1e3) / 1e12
+        line = {
+            "metric": METRIC, "value": total_q * world / (ms_graph / 1e3), "unit": "queries/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_graph, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": FORMS[precision].split("_")[0],
+            "data": "synthetic (seeded N(0,1) rounded to BF16, stored FP32)",
+            "config": {"workload": "batched_uneven", "databases": [{"N": n, "d": d} for n, d in dbs_spec],
+                       "batches": len(batches), "queries_per_step": total_q,
+                       "k_values": sorted({b[2] for b in batches}), "form": FORMS[precision],
+                       "l2": "databases (3.1 GB) larger than L2"},
+            "one_by_one": {"queries_per_s": total_q * world / (ms_loop / 1e3), "ms_per_step": ms_loop},
+            "batch_speedup": ms_loop / ms_graph,
+            "identical_to_alone": mismatches == 0, "items_differing": mismatches,
+            "recall_at_k_min_sampled": recall_min, "max_rel_dist_err_sampled": err_max,
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": p_form, "unit": "TFLOP/s",
+                         "frac": achieved / p_form, "traffic": None, "kernel": "whole graph (prep + fused + merge)",
+                         "peak_kind": peak_kind + " bf16 burst", "algorithmic": "sum 2*nq*N*d"},
+            "cpu_baseline": None,
+            "e2e": {"value": total_q * world / (ms_e2e / 1e3), "unit": "queries/s", "ms_per_step": ms_e2e,
+                    "h2d_bytes_per_step": sum(it[1].numel() * 4 for it in items),
+                    "d2h_bytes_per_step": sum(it[3].numel() * 8 for it in items)},
+            "gpu_launches": kernels * args.steps, "launches_per_step": {"graph": 1, "kernels_in_graph": kernels},
+            "workspace_bytes": ws_bytes,
+            "clocks": sampler.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    batch.close()
+    for ix, _ in dbs:
+        ix.close()
+    res.close()
+    barrier(world)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -199,12 +331,20 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--forms", default="0,1,2", help="precision forms to time (0 exact, 1 bf16, 2 fp8)")
     ap.add_argument("--no-recall", action="store_true", help="skip the oracle recall check (profiling runs)")
+    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, "batched_uneven"])
+    ap.add_argument("--batch-form", type=int, default=1, help="precision form of the batched workload")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_init()
     if args.impl == "reference":
         rc = run_reference(args, world, rank)
         barrier(world)
+        return rc
+    if args.workload == "batched_uneven":
+        rc = run_batched(args, world, rank, local)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return rc
 
     import numpy as np

@@ -22,7 +22,7 @@ import numpy as np
 
 __all__ = [
     "DeviceResources", "IndexBF", "IndexBFConfig", "MemorySpace", "Precision", "CurplshError",
-    "compute_l2_norm", "search_l2_distance", "lib_path", "get_num_devices",
+    "compute_l2_norm", "search_l2_distance", "lib_path", "get_num_devices", "SearchBatch",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -56,6 +56,12 @@ class _Cfg(ctypes.Structure):
                 ("store_transposed", ctypes.c_int32), ("compute_exact_distances", ctypes.c_int32),
                 ("precision", ctypes.c_int32), ("rerank_factor", ctypes.c_int32),
                 ("borrow_device_data", ctypes.c_int32)]
+
+
+class _BatchItem(ctypes.Structure):
+    _fields_ = [("index", ctypes.c_void_p), ("num", ctypes.c_int64), ("queries", ctypes.c_void_p),
+                ("k", ctypes.c_int32), ("pad0", ctypes.c_int32), ("indices", ctypes.c_void_p),
+                ("distances", ctypes.c_void_p)]
 
 
 def lib_path() -> str:
@@ -96,6 +102,10 @@ def _load():
         "curplsh_compute_l2_norm": (i32, [f32p, i64, i32, f32p, i32, vp]),
         "curplsh_search_l2_distance": (i32, [vp, f32p, i64, f32p, f32p, i64, i32, i32, i32p, f32p, i32]),
         "curplsh_index_search_noalloc": (i32, [vp, i64, f32p, i32, i32p, f32p, vp]),
+        "curplsh_batch_create": (i32, [ctypes.POINTER(_BatchItem), i32, i32, i32, ctypes.POINTER(vp)]),
+        "curplsh_batch_run": (i32, [vp, vp, i32]),
+        "curplsh_batch_get_info": (i32, [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int64)]),
+        "curplsh_batch_destroy": (i32, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -116,7 +126,8 @@ EXPORTED_SYMBOLS = (
     "curplsh_index_train", "curplsh_index_add", "curplsh_index_search", "curplsh_index_search_ex",
     "curplsh_index_search_profiled", "curplsh_index_reset", "curplsh_index_get_dimension",
     "curplsh_index_get_num_data", "curplsh_index_get_device", "curplsh_compute_l2_norm",
-    "curplsh_search_l2_distance", "curplsh_index_search_noalloc",
+    "curplsh_search_l2_distance", "curplsh_index_search_noalloc", "curplsh_batch_create", "curplsh_batch_run",
+    "curplsh_batch_get_info", "curplsh_batch_destroy",
 )
 
 
@@ -357,3 +368,52 @@ def search_l2_distance(resources: DeviceResources, bases, base_norms, queries, k
                                            _ptr(queries, np.float32), int(queries.shape[0]), int(queries.shape[1]),
                                            int(k), _ptr(indices, np.int32, True), _ptr(distances, np.float32, True),
                                            int(bool(exact_distances))))
+
+
+class SearchBatch:
+    """A fixed list of searches over one or more indexes, replayed as one CUDA graph.
+
+    ``items`` is a sequence of ``(index, queries, k, indices, distances)`` with
+    CUDA tensors on the indexes' device: queries [nq, dim] float32, indices
+    [nq, k] int32 and distances [nq, k] float32.  The tensors are captured by
+    address: overwrite ``queries`` in place and call :meth:`run` again.  Every
+    item's results equal ``index.search_ex`` of that item alone with the same
+    precision and rerank factor.  No counterpart in the reference.
+    """
+
+    def __init__(self, items, precision: int = -1, rerank_factor: int = -1):
+        arr = (_BatchItem * len(items))()
+        self._keep = []
+        for i, (index, queries, k, indices, distances) in enumerate(items):
+            nq = int(queries.shape[0])
+            arr[i].index = index._h
+            arr[i].num = nq
+            arr[i].queries = _ptr(queries, np.float32).value if nq else None
+            arr[i].k = int(k)
+            arr[i].indices = _ptr(indices, np.int32, True).value if nq else None
+            arr[i].distances = _ptr(distances, np.float32, True).value if nq else None
+            self._keep.append((index, queries, indices, distances))
+        h = ctypes.c_void_p()
+        _check(_lib.curplsh_batch_create(arr, len(items), int(precision), int(rerank_factor), ctypes.byref(h)))
+        self._h = h
+
+    def run(self, stream=None, wait: bool = True) -> None:
+        _check(_lib.curplsh_batch_run(self._h, _stream_ptr(stream), int(bool(wait))))
+
+    def info(self):
+        """(kernel launches per run, device working-memory bytes)."""
+        n = ctypes.c_int(0)
+        b = ctypes.c_int64(0)
+        _check(_lib.curplsh_batch_get_info(self._h, ctypes.byref(n), ctypes.byref(b)))
+        return n.value, b.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.curplsh_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

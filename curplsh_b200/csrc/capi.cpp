@@ -217,6 +217,7 @@ struct curplsh_index {
   uint8_t* x8 = nullptr;          // [n_pad x ld8]   (built on first FP8 search)
   float* xs = nullptr;            // [n_pad]
   uint32_t* status = nullptr;     // device error word
+  long long generation = 0;       // bumped whenever the prepared database changes (add, reset)
   std::map<cudaStream_t, std::unique_ptr<StreamWorkspace>> ws;
 
   void free_db() {
@@ -383,6 +384,8 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
   m.plan = plan;
   m.pools = pools;
   m.pool_counts = counts;
+  m.q_bound = qbound;
+  m.q_bound_half = qbound + nq_pad;
   m.queries = q_dev;
   m.db = ix->x32;
   m.ld_db = d;
@@ -524,9 +527,21 @@ int index_lock_view(curplsh_index* ix, IndexView* v) {
   v->xl = ix->xl;
   v->x8 = ix->x8;
   v->xs = ix->xs;
+  v->generation = ix->generation;
+  v->stream = ix->dres->def;
   return CURPLSH_OK;
 }
 void index_unlock(curplsh_index* ix) { ix->mu.unlock(); }
+int index_prepare_form(curplsh_index* ix, int form, IndexView* v) {
+  if (form != kFormFP8 || ix->x8 || ix->n == 0) return CURPLSH_OK;
+  DeviceScope scope(ix->cfg.device);
+  int rc = build_fp8(ix, ix->dres->def);
+  if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(ix->dres->def));
+  v->x8 = ix->x8;
+  v->xs = ix->xs;
+  return CURPLSH_OK;
+}
 int search_kprime(int form, int k, int rerank_factor, long long n) { return kprime_for(form, k, rerank_factor, n); }
 int search_pool_capacity(int kprime) { return pool_capacity(kprime); }
 int record_error(int code, const char* msg) { return set_error(code, "%s", msg); }
@@ -761,6 +776,7 @@ int curplsh_index_add(curplsh_index* ix, int64_t num, const float* data) {
   ix->xl = xl;
   ix->n = n_new;
   ix->n_pad = pad_new;
+  ++ix->generation;
   return CURPLSH_OK;
 }
 
@@ -788,6 +804,7 @@ int curplsh_index_reset(curplsh_index* ix) {
   cudaStreamSynchronize(ix->dres->def);
   for (auto& kv : ix->ws) cudaStreamSynchronize(kv.first);
   ix->free_db();
+  ++ix->generation;
   return CURPLSH_OK;
 }
 

@@ -86,8 +86,8 @@ struct FusedItem {
   int pool_cap;            // capacity of one candidate pool (entries)
   int num_qblocks;         // G_i = ceil(nq / 128)
   int num_tiles;           // T_i = ceil(nb / 256)
-  int units_per_block;     // U_i: max CTAs (units) that share one query block of this item
-  int pad0;
+  int units_per_block;     // U_i: max units (pool lists) of one query block of this item
+  int split_tiles;         // L_i: a unit never crosses a multiple of L_i tiles within its block
   long long work_begin;    // flattened offset of this item's first (block, tile)
   long long work_end;      // work_begin + G_i * T_i
   const float* db_norms;   // [nb_pad] squared norms, +inf for padding rows (FP8 form)

@@ -32,6 +32,8 @@
 #include <cstdio>
 
 #include "common.cuh"
+#include <algorithm>
+
 #include "fused_knn.h"
 #include "ptx.cuh"
 #include "select.cuh"
@@ -153,8 +155,13 @@ struct FusedArgs {
 };
 
 // Walks the contiguous range [cta*W, min(total,(cta+1)*W)) of the flattened
-// (item, query block, tile) space as units (item, query block, [t0, t1)).
-// u_ord numbers the CTAs that share one query block (0 = the first CTA).
+// (item, query block, tile) space as units (item, query block, [t0, t1)).  A
+// unit also ends at every multiple of the item's split length L, so no unit
+// gathers candidates from more than L tiles (a split-N knob: longer units
+// mean fewer pool lists for the merge but more in-pool selections).
+// u_ord numbers the units of one query block: the number of cuts (CTA range
+// starts and multiples of L) in (0, t0].  A position that is both kinds of
+// cut leaves one ordinal unused (`gap`): that unit writes zero counts for it.
 struct UnitWalk {
   long long pos, end, W;
   int ii;
@@ -163,18 +170,23 @@ struct UnitWalk {
     end = pos + W < B.total_work ? pos + W : B.total_work;
   }
   template <int MAXI>
-  __device__ bool next(int cta, const FusedArgs<MAXI>& A, int& item, int& qb, int& t0, int& t1, int& u_ord) {
+  __device__ bool next(const FusedArgs<MAXI>& A, int& item, int& qb, int& t0, int& t1, int& u_ord, bool& gap) {
     if (pos >= end) return false;
     while (ii < A.B.num_items && A.items[ii].work_end <= pos) ++ii;
     if (ii >= A.B.num_items) return false;
-    const long long wb = A.items[ii].work_begin;
-    const int T = A.items[ii].num_tiles;
+    const FusedItem& it = A.items[ii];
+    const long long wb = it.work_begin;
+    const int T = it.num_tiles;
+    const int Ls = it.split_tiles;
     const long long lp = pos - wb;
     qb = (int)(lp / T);
     t0 = (int)(lp - (long long)qb * T);
-    const long long len = (end - pos) < (long long)(T - t0) ? (end - pos) : (long long)(T - t0);
+    long long len = (end - pos) < (long long)(T - t0) ? (end - pos) : (long long)(T - t0);
+    if (len > (long long)(Ls - t0 % Ls)) len = Ls - t0 % Ls;
     t1 = t0 + (int)len;
-    u_ord = cta - (int)((wb + (long long)qb * T) / W);
+    const long long base = wb + (long long)qb * T;
+    u_ord = (int)(pos / W - base / W) + t0 / Ls;
+    gap = t0 > 0 && t0 % Ls == 0 && pos % W == 0;
     item = ii;
     pos += len;
     return true;
@@ -308,10 +320,11 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
       const uint64_t pol_q = l2_policy_evict_last();
       UnitWalk walk(blockIdx.x, B);
       int ii, qb, t0, t1, u_ord, unit = 0;
+      bool gap;
       uint32_t it = 0;
       bool ok = true;
       STAT_DECL(st_wait);
-      while (ok && walk.next(blockIdx.x, A, ii, qb, t0, t1, u_ord)) {
+      while (ok && walk.next(A, ii, qb, t0, t1, u_ord, gap)) {
         const CUtensorMap* mp = maps_of(ii);
         const CUtensorMap& tm_q_hi = mp[kMapQHi];
         const CUtensorMap& tm_q_lo = mp[kMapQLo];
@@ -375,11 +388,12 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
       constexpr uint32_t idesc = make_idesc(fmt, fmt, kBM, kBN);
       UnitWalk walk(blockIdx.x, B);
       int ii, qb, t0, t1, u_ord, unit = 0;
+      bool gap;
       uint32_t it = 0, tc = 0;
       bool ok = true;
       STAT_DECL(st_full);
       STAT_DECL(st_acc);
-      while (ok && walk.next(blockIdx.x, A, ii, qb, t0, t1, u_ord)) {
+      while (ok && walk.next(A, ii, qb, t0, t1, u_ord, gap)) {
         if (!L.a_stream) {
           if (!wait_or_abort(a_full, unit & 1, abort_flag)) {
             raise_abort(abort_flag, B.status, kErrWaitTimeout);
@@ -459,6 +473,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
     const uint32_t lane_base = (uint32_t)(lg * 32) << 16;
     UnitWalk walk(blockIdx.x, B);
     int ii, qb, t0, t1, u_ord;
+    bool gap;
     uint32_t tc = 0;
     bool ok = true;
     STAT_DECL(st_wait);
@@ -472,7 +487,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
 #ifdef CURPLSH_FUSED_STATS
     if (threadIdx.x == 64 && B.stats) g_radix_pass_counter = &B.stats[kStatRadixPasses];
 #endif
-    while (ok && walk.next(blockIdx.x, A, ii, qb, t0, t1, u_ord)) {
+    while (ok && walk.next(A, ii, qb, t0, t1, u_ord, gap)) {
       const FusedItem& p = A.items[ii];
       const int P = p.pool_cap;
       const int U = p.units_per_block;
@@ -663,7 +678,10 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
       refresh(__ballot_sync(0xffffffffu, n > p.kprime), p.kprime);
       // a refresh may keep a few more than k' keys (unsorted): record them all;
       // the merge pass selects exactly
-      if (valid) p.pool_counts[((pool_row0 + row) * U + u_ord) * 2 + g] = n < P ? n : P;
+      if (valid) {
+        p.pool_counts[((pool_row0 + row) * U + u_ord) * 2 + g] = n < P ? n : P;
+        if (gap) p.pool_counts[((pool_row0 + row) * U + u_ord - 1) * 2 + g] = 0;
+      }
     }
     if (lane == 0) {
       STAT_FLUSH(kStatEpiWaitAccFull, st_wait);
@@ -726,18 +744,26 @@ bool make_map(CUtensorMap* m, const void* base, bool fp8, long long rows, long l
   return r == CUDA_SUCCESS;
 }
 
+// Raises the kernel's dynamic shared memory limit once per device.
 template <int FORM, int MAXI>
-cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, int n, const FusedBatchPlan& bp,
-                        uint32_t* status, unsigned long long* stats, uint32_t smem, cudaStream_t st) {
-  static bool attr_done[16] = {};
+cudaError_t ensure_attributes() {
+  static bool attr_done[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
-  if (!attr_done[dev & 15]) {
+  if (!attr_done[dev & 63]) {
     cudaError_t e = cudaFuncSetAttribute(fused_knn_kernel<FORM, MAXI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          227 * 1024);
     if (e != cudaSuccess) return e;
-    attr_done[dev & 15] = true;
+    attr_done[dev & 63] = true;
   }
+  return cudaSuccess;
+}
+
+template <int FORM, int MAXI>
+cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, int n, const FusedBatchPlan& bp,
+                        uint32_t* status, unsigned long long* stats, uint32_t smem, cudaStream_t st) {
+  cudaError_t e = ensure_attributes<FORM, MAXI>();
+  if (e != cudaSuccess) return e;
   FusedArgs<MAXI> a;
   memset(&a, 0, sizeof(a));
   a.B.num_items = n;
@@ -759,6 +785,7 @@ cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, 
     it.num_qblocks = pl.num_qblocks;
     it.num_tiles = pl.num_tiles;
     it.units_per_block = pl.units_per_block;
+    it.split_tiles = pl.split_tiles;
     it.work_begin = pl.work_begin;
     it.work_end = pl.work_end;
     it.db_norms = f.xn;
@@ -811,6 +838,8 @@ void plan_fused_batch(const FusedItemSpec* specs, int n, int max_ctas, FusedItem
     FusedItemPlan& pl = plans[i];
     pl.num_qblocks = specs[i].nb > 0 ? (specs[i].nq + kBM - 1) / kBM : 0;
     pl.num_tiles = (specs[i].nb + kBN - 1) / kBN;
+    pl.split_tiles = specs[i].split_tiles > 0 && specs[i].split_tiles < pl.num_tiles ? specs[i].split_tiles
+                                                                                      : std::max(pl.num_tiles, 1);
     pl.work_begin = total;
     total += (long long)pl.num_qblocks * pl.num_tiles;
     pl.work_end = total;
@@ -825,9 +854,9 @@ void plan_fused_batch(const FusedItemSpec* specs, int n, int max_ctas, FusedItem
     FusedItemPlan& pl = plans[i];
     int U = 1;
     for (int qb = 0; qb < pl.num_qblocks; ++qb) {
-      const long long first = (pl.work_begin + (long long)qb * pl.num_tiles) / W;
-      const long long last = (pl.work_begin + (long long)(qb + 1) * pl.num_tiles - 1) / W;
-      if (last - first + 1 > U) U = (int)(last - first + 1);
+      const long long base = pl.work_begin + (long long)qb * pl.num_tiles;
+      const long long u = (base + pl.num_tiles - 1) / W - base / W + (pl.num_tiles - 1) / pl.split_tiles + 1;
+      if (u > U) U = (int)u;
     }
     pl.units_per_block = U;
   }
@@ -848,6 +877,23 @@ void plan_fused(int nq, int nb, int num_sms, FusedPlan* out) {
 }
 
 uint32_t fused_smem_bytes(int form, int d) { return make_layout(form, d).total; }
+
+cudaError_t prepare_fused_kernels(int form) {
+  cudaError_t e;
+  switch (form) {
+    case kFormExact:
+      e = ensure_attributes<kFormExact, 1>();
+      return e != cudaSuccess ? e : ensure_attributes<kFormExact, kFusedMaxItems>();
+    case kFormBF16:
+      e = ensure_attributes<kFormBF16, 1>();
+      return e != cudaSuccess ? e : ensure_attributes<kFormBF16, kFusedMaxItems>();
+    case kFormFP8:
+      e = ensure_attributes<kFormFP8, 1>();
+      return e != cudaSuccess ? e : ensure_attributes<kFormFP8, kFusedMaxItems>();
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
 
 cudaError_t launch_fused_batch(int form, const FusedItemSpec* specs, const FusedItemPlan* plans, int n,
                                const FusedBatchPlan& bp, uint32_t* status, unsigned long long* stats,
@@ -898,6 +944,7 @@ cudaError_t launch_fused(const FusedLaunch& f, cudaStream_t st) {
   ip.num_qblocks = f.plan.num_qblocks;
   ip.num_tiles = f.plan.num_tiles;
   ip.units_per_block = f.plan.units_per_block;
+  ip.split_tiles = std::max(f.plan.num_tiles, 1);
   ip.work_begin = 0;
   ip.work_end = (long long)f.plan.num_qblocks * f.plan.num_tiles;
   FusedBatchPlan bp;

@@ -53,6 +53,7 @@ constexpr int kFusedMaxItems = 16;
 
 struct FusedItemSpec {
   int nq, nb, d, kprime, pool_cap;
+  int split_tiles;  // max tiles per unit (<= 0: no limit beyond the CTA ranges)
   long long nq_pad, nb_pad, ld16, ld8;
   const __nv_bfloat16* qh;
   const __nv_bfloat16* ql;
@@ -71,16 +72,20 @@ struct FusedItemSpec {
 };
 struct FusedItemPlan {
   int num_qblocks, num_tiles, units_per_block;
+  int split_tiles;  // resolved split length L (>= 1)
   long long work_begin, work_end;
 };
 struct FusedBatchPlan {
   long long total_work = 0, work_per_cta = 1;
   int grid = 0;
 };
-// Plans `n` items over at most `max_ctas` CTAs.  Only nq and nb of the specs
-// are read, so pool sizes (which depend on units_per_block) can be computed
+// Plans `n` items over at most `max_ctas` CTAs.  Only nq, nb and split_tiles
+// of the specs are read, so pool sizes (which depend on units_per_block) can be computed
 // from the plan before the pools are carved.
 void plan_fused_batch(const FusedItemSpec* specs, int n, int max_ctas, FusedItemPlan* plans, FusedBatchPlan* out);
+// Sets the kernels' launch attributes on the current device (done lazily by
+// the launches; call it before a stream capture).
+cudaError_t prepare_fused_kernels(int form);
 cudaError_t launch_fused_batch(int form, const FusedItemSpec* specs, const FusedItemPlan* plans, int n,
                                const FusedBatchPlan& bp, uint32_t* status, unsigned long long* stats,
                                cudaStream_t st);
@@ -122,6 +127,8 @@ struct MergeLaunch {
   FusedPlan plan;
   const uint64_t* pools;
   const int* pool_counts;
+  const uint32_t* q_bound;       // final bounds of the fused pass (may be null)
+  const uint32_t* q_bound_half;  // [nq_pad][2]
   const float* queries;   // [nq x d] fp32, row stride d
   const float* db;        // [nb x d] fp32, row stride ld_db
   long long ld_db;
@@ -139,12 +146,14 @@ constexpr int kMergeMaxItems = 128;
 struct MergeItem {
   int nq, k, kprime, pool_cap, num_tiles, units_per_block;
   int row0;                // first pool row of this item within its fused item
-  int pad0;
+  int split_tiles;         // the fused item's resolved split length L
   long long work_begin;    // the fused item's offset in its launch's flattened work space
   long long work_per_cta;  // W of that launch
   long long q_begin;       // first CTA of this item (filled by launch_merge_batch)
   const uint64_t* pools;   // the fused item's pools and counts
   const int* pool_counts;
+  const uint32_t* q_bound;       // the fused item's final bounds by pool row (may be null)
+  const uint32_t* q_bound_half;  // [rows][2]
   const float* queries;    // [nq x d] fp32, row stride d
   const float* db;         // database rows fp32, row stride ld_db
   long long ld_db;
@@ -152,6 +161,7 @@ struct MergeItem {
   float* out_dist;
 };
 cudaError_t launch_merge_batch(MergeItem* items, int n, int d, uint32_t* status, cudaStream_t st);
+cudaError_t prepare_merge_kernel();
 
 // Fill [n] ints / floats (N == 0 results, padding).
 cudaError_t launch_fill_results(int* idx, float* dist, long long n, cudaStream_t st);
@@ -172,10 +182,15 @@ struct IndexView {
   const __nv_bfloat16* xl;
   const uint8_t* x8;
   const float* xs;
+  long long generation;  // changes whenever add()/reset() replace the prepared database
+  cudaStream_t stream;   // the index's default stream
 };
 // Locks the index (same lock as search/add) and fills `out`; unlock with index_unlock.
 int index_lock_view(curplsh_index* index, IndexView* out);
 void index_unlock(curplsh_index* index);
+// With the lock held: builds the FP8 copy if `form` needs it and it is missing
+// (synchronous), updating `v`.
+int index_prepare_form(curplsh_index* index, int form, IndexView* v);
 // Candidate count k' and pool capacity used by every search of this library.
 int search_kprime(int form, int k, int rerank_factor, long long n);
 int search_pool_capacity(int kprime);

@@ -14,6 +14,7 @@
 //   3. bitonic sort by (exact distance, row) -- lower row first on ties -- and
 //      write the first k; missing results are (-1, FLT_MAX) as in
 //      src/internal/search.cu:94-101.
+#include <algorithm>
 #include <cstring>
 
 #include "common.cuh"
@@ -43,10 +44,48 @@ __device__ __forceinline__ uint32_t block_incl_scan(uint32_t v, uint32_t* warp_t
 struct MergeArgs {
   MergeItem items[kMergeMaxItems];
   int num_items, d;
-  int kp2;     // power of two >= the largest kprime
-  int lcnt_n;  // room for the largest 2 * units_per_block, rounded to 4
+  int kp2;      // power of two >= the largest kprime
+  int pre_cap;  // capacity of the prefiltered key buffer (2 * kp2)
+  int lcnt_n;   // room for the largest list count, rounded to 4
+  int vec4;     // query and database rows allow 16-byte loads
   uint32_t* status;
 };
+
+// Block-wide radix select: the bound B such that exactly `keep` of the keys
+// visited by `each` are <= B (keys are unique).  `each(f)` calls f(key) for
+// every key of this thread's share.  8-bit digits from the top; stops as soon
+// as the digit bucket holds exactly the remaining rank.
+template <class Each>
+__device__ uint64_t block_select_bound(Each each, uint32_t keep, uint32_t* hist, uint32_t* warp_tot,
+                                       uint32_t* misc) {
+  const int tid = threadIdx.x;
+  uint64_t prefix = 0, pmask = 0;
+  uint32_t rank = keep;
+  for (int shift = 56; shift >= 0; shift -= 8) {
+    hist[tid] = 0u;  // kMergeThreads == 256 bins
+    __syncthreads();
+    each([&](uint64_t key) {
+      if ((key & pmask) == prefix) atomicAdd(&hist[(uint32_t)(key >> shift) & 255u], 1u);
+    });
+    __syncthreads();
+    const uint32_t c = hist[tid];
+    const uint32_t incl = block_incl_scan(c, warp_tot);
+    const uint32_t excl = incl - c;
+    if (excl < rank && rank <= incl) {
+      misc[1] = (uint32_t)tid;
+      misc[2] = excl;
+      misc[3] = c;
+    }
+    __syncthreads();
+    const uint32_t digit = misc[1], before = misc[2], cnt = misc[3];
+    prefix |= (uint64_t)digit << shift;
+    pmask |= 0xFFull << shift;
+    rank -= before;
+    __syncthreads();
+    if (cnt == rank || shift == 0) return prefix | ~pmask;
+  }
+  return ~0ull;
+}
 
 __global__ void __launch_bounds__(kMergeThreads) merge_rerank_kernel(const __grid_constant__ MergeArgs a) {
   int lo = 0, hi = a.num_items - 1;  // last item with q_begin <= blockIdx.x
@@ -57,18 +96,18 @@ __global__ void __launch_bounds__(kMergeThreads) merge_rerank_kernel(const __gri
     else
       hi = mid - 1;
   }
-  const int ii = lo;
-  const MergeItem& m = a.items[ii];
+  const MergeItem& m = a.items[lo];
   const int q = (int)((long long)blockIdx.x - m.q_begin);
   if (q >= m.nq) return;
   const int d = a.d;
   extern __shared__ __align__(16) uint8_t sm[];
-  uint64_t* cand = reinterpret_cast<uint64_t*>(sm);                       // [kp2]
-  uint32_t* hist = reinterpret_cast<uint32_t*>(cand + a.kp2);             // [256]
-  uint32_t* warp_tot = hist + 256;                                         // [8]
-  uint32_t* misc = warp_tot + 8;                                           // [8]
-  int* lcnt = reinterpret_cast<int*>(misc + 8);                            // [lcnt_n]
-  float* qv = reinterpret_cast<float*>(lcnt + a.lcnt_n);                   // [d]
+  uint64_t* cand = reinterpret_cast<uint64_t*>(sm);             // [kp2] kept keys, then reranked keys
+  uint64_t* pre = cand + a.kp2;                                 // [pre_cap] keys that pass the final bound
+  uint32_t* hist = reinterpret_cast<uint32_t*>(pre + a.pre_cap);  // [256]
+  uint32_t* warp_tot = hist + 256;                              // [8]
+  uint32_t* misc = warp_tot + 8;                                // [8]
+  int* lcnt = reinterpret_cast<int*>(misc + 8);                 // [lcnt_n]
+  float* qv = reinterpret_cast<float*>(lcnt + a.lcnt_n);        // [d], 16-byte aligned
 
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
@@ -78,100 +117,139 @@ __global__ void __launch_bounds__(kMergeThreads) merge_rerank_kernel(const __gri
   const long long W = m.work_per_cta;
   const long long first = (m.work_begin + (long long)qb * T) / W;
   const long long last = (m.work_begin + (long long)(qb + 1) * T - 1) / W;
-  const int nlists = T > 0 ? 2 * (int)(last - first + 1) : 0;  // an empty database has no pools
+  // an empty database has no pools; otherwise one list per unit and half
+  const int nlists = T > 0 ? 2 * (int)(last - first + 1 + (T - 1) / m.split_tiles) : 0;
   const size_t list0 = ((size_t)qb * kBM + row) * U * 2;  // pool-list index of (u=0, h=0)
+  // Final bound of the fused pass on this query's k'-th coarse distance: the
+  // smallest k'-th of any pool, and the larger of the per-half (k'/2)-th
+  // bounds.  Every key of the k' smallest has a distance <= it.
+  uint32_t qbound = 0xFFFFFFFFu;
+  if (m.q_bound && T > 0 && a.pre_cap > 0) {
+    const uint32_t h0 = m.q_bound_half[2 * (size_t)prow], h1 = m.q_bound_half[2 * (size_t)prow + 1];
+    qbound = min(m.q_bound[prow], max(h0, h1));
+  }
 
   for (int i = tid; i < d; i += kMergeThreads) qv[i] = m.queries[(size_t)q * d + i];
-  if (tid == 0) misc[0] = 0;
+  if (tid == 0) {
+    misc[0] = 0;
+    misc[4] = 0;
+  }
   for (int l = tid; l < nlists; l += kMergeThreads) lcnt[l] = m.pool_counts[list0 + l];
   __syncthreads();
-  int total = 0;
-  for (int l = 0; l < nlists; ++l) total += lcnt[l];
-  const int keep = total < m.kprime ? total : m.kprime;
-
   auto list_ptr = [&](int l) { return m.pools + (list0 + (size_t)l) * (size_t)m.pool_cap; };
-
-  // ---- 1. radix-select the k' smallest keys (skipped when everything fits)
-  uint64_t bound = ~0ull;
-  if (total > keep) {
-    uint64_t prefix = 0, pmask = 0;
-    uint32_t rank = (uint32_t)keep;
-    for (int shift = 56; shift >= 0; shift -= 8) {
-      hist[tid] = 0u;  // kMergeThreads == 256 bins
-      __syncthreads();
-      for (int l = 0; l < nlists; ++l) {
-        const uint64_t* lp = list_ptr(l);
-        for (int o = tid; o < lcnt[l]; o += kMergeThreads) {
-          const uint64_t key = lp[o];
-          if ((key & pmask) == prefix) atomicAdd(&hist[(uint32_t)(key >> shift) & 255u], 1u);
-        }
-      }
-      __syncthreads();
-      const uint32_t c = hist[tid];
-      const uint32_t incl = block_incl_scan(c, warp_tot);
-      const uint32_t excl = incl - c;
-      if (excl < rank && rank <= incl) {
-        misc[1] = (uint32_t)tid;
-        misc[2] = excl;
-        misc[3] = c;
-      }
-      __syncthreads();
-      const uint32_t digit = misc[1], before = misc[2], cnt = misc[3];
-      prefix |= (uint64_t)digit << shift;
-      pmask |= 0xFFull << shift;
-      rank -= before;
-      __syncthreads();
-      if (cnt == rank || shift == 0) {
-        bound = prefix | ~pmask;
-        break;
+  auto each_pool_key = [&](auto f) {
+    for (int l = 0; l < nlists; ++l) {
+      const uint64_t* lp = list_ptr(l);
+      for (int o = tid; o < lcnt[l]; o += kMergeThreads) {
+        const uint64_t key = lp[o];
+        if ((uint32_t)(key >> 32) <= qbound) f(key);
       }
     }
+  };
+
+  // ---- 1. keys under the final bound, compacted into shared memory (when
+  // this launch's pools can carry bounds at all)
+  int cnt = 0;
+  if (a.pre_cap > 0) {
+    each_pool_key([&](uint64_t key) {
+      const uint32_t pos = atomicAdd(&misc[0], 1u);
+      if (pos < (uint32_t)a.pre_cap) pre[pos] = key;
+    });
+    __syncthreads();
+    cnt = (int)misc[0];
+  } else {
+    for (int l = 0; l < nlists; ++l) cnt += lcnt[l];
   }
-  // ---- gather the kept keys
-  for (int l = 0; l < nlists; ++l) {
-    const uint64_t* lp = list_ptr(l);
-    for (int o = tid; o < lcnt[l]; o += kMergeThreads) {
-      const uint64_t key = lp[o];
+  const int keep = cnt < m.kprime ? cnt : m.kprime;
+  // ---- 2. select the k' smallest (in shared memory unless too many passed)
+  uint64_t bound = ~0ull;
+  if (cnt <= a.pre_cap) {
+    if (cnt > keep)
+      bound = block_select_bound(
+          [&](auto f) {
+            for (int i = tid; i < cnt; i += kMergeThreads) f(pre[i]);
+          },
+          (uint32_t)keep, hist, warp_tot, misc);
+    for (int i = tid; i < cnt; i += kMergeThreads) {
+      const uint64_t key = pre[i];
       if (key <= bound) {
-        const uint32_t pos = atomicAdd(&misc[0], 1u);
+        const uint32_t pos = atomicAdd(&misc[4], 1u);
         if (pos < (uint32_t)a.kp2) cand[pos] = key;
       }
     }
+  } else {
+    if (cnt > keep) bound = block_select_bound(each_pool_key, (uint32_t)keep, hist, warp_tot, misc);
+    each_pool_key([&](uint64_t key) {
+      if (key <= bound) {
+        const uint32_t pos = atomicAdd(&misc[4], 1u);
+        if (pos < (uint32_t)a.kp2) cand[pos] = key;
+      }
+    });
   }
   __syncthreads();
-  int kept = (int)misc[0];
+  int kept = (int)misc[4];
   if (kept > a.kp2) {
     if (tid == 0) atomicOr(a.status, kErrPoolOverflow);
     kept = a.kp2;
   }
-  // ---- 2. exact FP32 rerank, one warp per candidate
-  for (int c = warp; c < kept; c += kMergeThreads / 32) {
-    const uint32_t idx = (uint32_t)(cand[c] & 0xFFFFFFFFu);
-    const float* xr = m.db + (size_t)idx * m.ld_db;
-    float s = 0.f;
-    for (int i = lane; i < d; i += 32) {
-      const float t = qv[i] - __ldg(xr + i);
-      s = fmaf(t, t, s);
+  // ---- 3. exact FP32 rerank: one warp per pair of candidates (two rows in
+  // flight), lane-strided partial sums then a butterfly (fixed order)
+  for (int c = 2 * warp; c < kept; c += 2 * (kMergeThreads / 32)) {
+    const bool two = c + 1 < kept;
+    const uint32_t i0 = (uint32_t)(cand[c] & 0xFFFFFFFFu);
+    const uint32_t i1 = two ? (uint32_t)(cand[c + 1] & 0xFFFFFFFFu) : i0;
+    const float* x0 = m.db + (size_t)i0 * m.ld_db;
+    const float* x1 = m.db + (size_t)i1 * m.ld_db;
+    float s0 = 0.f, s1 = 0.f;
+    if (a.vec4) {
+      const float4* q4 = reinterpret_cast<const float4*>(qv);
+      const float4* y0 = reinterpret_cast<const float4*>(x0);
+      const float4* y1 = reinterpret_cast<const float4*>(x1);
+      for (int i = lane; i < d / 4; i += 32) {
+        const float4 qq = q4[i], u = __ldg(y0 + i), v = __ldg(y1 + i);
+        float t;
+        t = qq.x - u.x; s0 = fmaf(t, t, s0);
+        t = qq.y - u.y; s0 = fmaf(t, t, s0);
+        t = qq.z - u.z; s0 = fmaf(t, t, s0);
+        t = qq.w - u.w; s0 = fmaf(t, t, s0);
+        t = qq.x - v.x; s1 = fmaf(t, t, s1);
+        t = qq.y - v.y; s1 = fmaf(t, t, s1);
+        t = qq.z - v.z; s1 = fmaf(t, t, s1);
+        t = qq.w - v.w; s1 = fmaf(t, t, s1);
+      }
+    } else {
+      for (int i = lane; i < d; i += 32) {
+        const float qq = qv[i];
+        const float t0 = qq - __ldg(x0 + i), t1 = qq - __ldg(x1 + i);
+        s0 = fmaf(t0, t0, s0);
+        s1 = fmaf(t1, t1, s1);
+      }
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) cand[c] = make_key(s, idx);
+    for (int o = 16; o > 0; o >>= 1) {
+      s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    }
+    if (lane == 0) {
+      cand[c] = make_key(s0, i0);
+      if (two) cand[c + 1] = make_key(s1, i1);
+    }
   }
   for (int c = kept + tid; c < a.kp2; c += kMergeThreads) cand[c] = kKeyEmpty;
   __syncthreads();
-  // ---- 3. bitonic sort by (exact distance, row)
+  // ---- 4. bitonic sort by (exact distance, row)
   int n2 = 1;
   while (n2 < kept) n2 <<= 1;
   for (int size = 2; size <= n2; size <<= 1) {
     for (int stride = size >> 1; stride > 0; stride >>= 1) {
       for (int i = tid; i < n2 / 2; i += kMergeThreads) {
-        const int lo = 2 * i - (i & (stride - 1));
-        const int hi = lo + stride;
-        const bool asc = (lo & size) == 0;
-        const uint64_t x = cand[lo], y = cand[hi];
+        const int lo2 = 2 * i - (i & (stride - 1));
+        const int hi2 = lo2 + stride;
+        const bool asc = (lo2 & size) == 0;
+        const uint64_t x = cand[lo2], y = cand[hi2];
         if ((x > y) == asc) {
-          cand[lo] = y;
-          cand[hi] = x;
+          cand[lo2] = y;
+          cand[hi2] = x;
         }
       }
       __syncthreads();
@@ -192,6 +270,19 @@ __global__ void __launch_bounds__(kMergeThreads) merge_rerank_kernel(const __gri
 
 }  // namespace
 
+cudaError_t prepare_merge_kernel() {
+  static bool attr_done[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_done[dev & 63]) {
+    cudaError_t e =
+        cudaFuncSetAttribute(merge_rerank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e != cudaSuccess) return e;
+    attr_done[dev & 63] = true;
+  }
+  return cudaSuccess;
+}
+
 cudaError_t launch_merge_batch(MergeItem* items, int n, int d, uint32_t* status, cudaStream_t st) {
   if (n < 1 || n > kMergeMaxItems) return cudaErrorInvalidValue;
   MergeArgs a;
@@ -209,20 +300,28 @@ cudaError_t launch_merge_batch(MergeItem* items, int n, int d, uint32_t* status,
   a.num_items = n;
   a.d = d;
   a.status = status;
-  int kp2 = 1;
+  int kp2 = 32;  // >= 32 keeps the shared-memory carve 16-byte aligned
   while (kp2 < kpmax) kp2 <<= 1;
   a.kp2 = kp2;
-  a.lcnt_n = (2 * umax + 3) & ~3;
-  const size_t smem = (size_t)kp2 * 8 + (256 + 8 + 8) * 4 + (size_t)a.lcnt_n * 4 + (size_t)d * 4 + 16;
-  static bool attr_done[16] = {};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (!attr_done[dev & 15]) {
-    cudaError_t e =
-        cudaFuncSetAttribute(merge_rerank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    if (e != cudaSuccess) return e;
-    attr_done[dev & 15] = true;
+  // A pool can bound the k'-th distance only if a unit's half covers at least
+  // k' rows; without such pools there is nothing to prefilter with, and the
+  // launch keeps the smaller shared-memory footprint (higher occupancy).
+  bool bounded = false;
+  for (int i = 0; i < n; ++i) {
+    long long len = std::min<long long>(items[i].split_tiles, items[i].work_per_cta);
+    len = std::min<long long>(len, items[i].num_tiles);
+    bounded = bounded || (items[i].q_bound && len * kHalfN >= items[i].kprime);
   }
+  a.pre_cap = bounded ? 2 * kp2 : 0;
+  a.lcnt_n = (2 * umax + 3) & ~3;
+  bool vec4 = d % 4 == 0;
+  for (int i = 0; i < n; ++i)
+    vec4 = vec4 && (reinterpret_cast<uintptr_t>(items[i].queries) & 15) == 0 &&
+           (reinterpret_cast<uintptr_t>(items[i].db) & 15) == 0 && items[i].ld_db % 4 == 0;
+  a.vec4 = vec4 ? 1 : 0;
+  const size_t smem = (size_t)(a.kp2 + a.pre_cap) * 8 + (256 + 8 + 8) * 4 + (size_t)a.lcnt_n * 4 + (size_t)d * 4 + 16;
+  cudaError_t e = prepare_merge_kernel();
+  if (e != cudaSuccess) return e;
   if (smem > 200 * 1024 || qsum > 0x7fffffffLL) return cudaErrorInvalidValue;
   merge_rerank_kernel<<<(unsigned)qsum, kMergeThreads, smem, st>>>(a);
   return cudaGetLastError();
@@ -238,10 +337,13 @@ cudaError_t launch_merge_rerank(const MergeLaunch& m, cudaStream_t st) {
   it.num_tiles = m.plan.num_tiles;
   it.units_per_block = m.plan.units_per_block;
   it.row0 = 0;
+  it.split_tiles = m.plan.num_tiles > 0 ? m.plan.num_tiles : 1;
   it.work_begin = 0;
   it.work_per_cta = m.plan.work_per_cta;
   it.pools = m.pools;
   it.pool_counts = m.pool_counts;
+  it.q_bound = m.q_bound;
+  it.q_bound_half = m.q_bound_half;
   it.queries = m.queries;
   it.db = m.db;
   it.ld_db = m.ld_db;

@@ -220,6 +220,8 @@ int search_noalloc_locked(const IndexView& v, int nq, const float* q, int k, int
   m.plan = plan;
   m.pools = pools;
   m.pool_counts = counts;
+  m.q_bound = qbound;
+  m.q_bound_half = qbound + nq_pad;
   m.queries = q;
   m.db = v.x32;
   m.ld_db = v.dim;

@@ -71,6 +71,40 @@ def sphere_mixture(n: int, q: int, d: int = 96, centroids: int = 4096, sigma: fl
     return draw(n), draw(q)
 
 
+def batched_uneven_spec(seed: int = 3, num_dbs: int = 8, num_batches: int = 64, n_lo: int = 10_000,
+                        n_hi: int = 2_000_000, q_lo: int = 1, q_hi: int = 4096, dims=(64, 128, 256, 512),
+                        ks=(1, 10, 100, 1024)):
+    """Shapes of the uneven batched workload: `num_dbs` resident databases with
+    N log-uniform in [n_lo, n_hi] and d cycling through a shuffled `dims` (so
+    every dimension occurs); `num_batches` query
+    batches with sizes log-uniform in [q_lo, q_hi], each against a random
+    database with k drawn from `ks`.  Returns (dbs [(n, d)], batches [(db, nq, k)])."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    dbs = []
+    dim_order = [int(x) for x in rng.permutation(list(dims) * ((num_dbs + len(dims) - 1) // len(dims)))]
+    for i in range(num_dbs):
+        n = int(round(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi)))))
+        dbs.append((n, dim_order[i]))
+    batches = []
+    for _ in range(num_batches):
+        nq = int(round(np.exp(rng.uniform(np.log(q_lo), np.log(q_hi)))))
+        db = int(rng.integers(num_dbs))
+        k = int(rng.choice(ks))
+        batches.append((db, nq, min(k, dbs[db][0])))
+    return dbs, batches
+
+
+def normal_bf16(rows: int, d: int, seed: int, device="cuda", chunk: int = 1 << 20):
+    """i.i.d. N(0,1) values rounded to BF16, stored FP32."""
+    g = _gen(device, seed)
+    out = torch.empty((rows, d), device=device)
+    for s in range(0, rows, chunk):
+        e = min(rows, s + chunk)
+        out[s:e] = torch.randn((e - s, d), generator=g, device=device).bfloat16().float()
+    return out
+
+
 def make(name: str, device="cuda", n: int | None = None, q: int | None = None):
     """Inputs of a named configuration (optionally with N or Q overridden)."""
     N, Q, d, k = CONFIGS[name]

@@ -159,6 +159,41 @@ int curplsh_search_l2_distance(curplsh_resources* res, const float* bases, int64
                                const float* queries, int64_t nq, int dim, int k, int* indices,
                                float* distances, int exact_distances);
 
+/* ------------------------------------------------------------ batched search */
+/* No counterpart in the reference (its IndexBF::search serves one query matrix against one index
+ * per call, src/index_bf.cpp:46-74).  A batch is a fixed list of (index, queries, k, outputs)
+ * items, possibly over several indexes of different dimensions, planned once and replayed as ONE
+ * CUDA graph launch: per (precision form, dimension) group one segmented query-prep kernel, one
+ * persistent fused filter kernel whose balanced schedule spans every item of the group (several
+ * small query batches against the same index share query blocks), and one merge + rerank kernel;
+ * the groups run as parallel branches of the graph.  Each item's results are the same as curplsh_index_search_ex of that item alone with
+ * the same precision and rerank factor. */
+typedef struct curplsh_batch curplsh_batch;
+
+typedef struct curplsh_batch_item {
+  curplsh_index* index;
+  int64_t num;           /* queries in this item (0 allowed) */
+  const float* queries;  /* device [num x dim] of the index's device */
+  int32_t k;             /* 1..1024 */
+  int32_t pad0;
+  int32_t* indices;      /* device [num x k] */
+  float* distances;      /* device [num x k] */
+} curplsh_batch_item;
+
+/* Plans the batch (the pointers are captured: keep them valid and overwrite their contents
+ * between runs), allocates its working memory and captures the graph.  precision -1 and
+ * rerank_factor <= 0 take each index's default.  All indexes must live on one device.  Must not
+ * be called while the calling thread captures a stream. */
+int curplsh_batch_create(const curplsh_batch_item* items, int count, int precision, int rerank_factor,
+                         curplsh_batch** out);
+/* Launches the graph on `stream` (NULL: the first index's default stream).  wait != 0 synchronises
+ * and checks the device status word.  An index changed by add()/reset() since the last plan is
+ * re-planned (and the graph re-captured) first. */
+int curplsh_batch_run(curplsh_batch* batch, void* stream, int wait);
+/* Kernel launches in one run of the graph, and bytes of device working memory held. */
+int curplsh_batch_get_info(const curplsh_batch* batch, int* kernel_launches, int64_t* workspace_bytes);
+int curplsh_batch_destroy(curplsh_batch* batch);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif
