@@ -222,14 +222,38 @@ def run_batched(args, world, rank, local):
         q = synth.normal_bf16(nq, x.shape[1], seed=1000 + j + 7919 * rank, device=dev)
         items.append((ix, q, k, torch.empty((nq, k), dtype=torch.int32, device=dev),
                       torch.empty((nq, k), dtype=torch.float32, device=dev)))
+    torch.cuda.synchronize()  # the inputs were generated on torch's stream; the library uses its own
     total_q = sum(it[1].shape[0] for it in items)
     flops = sum(2.0 * it[1].shape[0] * dbs[b[0]][1].shape[0] * it[1].shape[1] for it, b in zip(items, batches))
+    tuned = None
+    if args.tune:
+        # one-time autotuning of every bucket the batch looks up (outside the timed region)
+        from curplsh_b200 import autotune
+        cb.tuning_clear()
+        untuned = cb.SearchBatch(items, precision=precision)
+        for _ in range(args.warmup):
+            untuned.run(stream=stream, wait=False)
+        stream.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            untuned.run(stream=stream, wait=False)
+        e1.record(stream)
+        e1.synchronize()
+        untuned.close()
+        t0 = time.perf_counter()
+        recs = autotune.tune_batch(items, precision=precision, reps=2, stream=stream)
+        tuned = {"buckets": len(recs), "tuning_s": time.perf_counter() - t0,
+                 "untuned_ms_per_step": e0.elapsed_time(e1) / args.steps,
+                 "changed": sum(1 for r in recs if (r["split_q4"], r["pool_headroom"]) != autotune.DEFAULT)}
     batch = cb.SearchBatch(items, precision=precision)
     kernels, ws_bytes = batch.info()
     # correctness: every item equals its search alone; a query sample against the oracle
     batch.run(stream=stream)
     mismatches = 0
     recall_min, err_max = 1.0, 0.0
+    recall_failures = []
     for j, (ix, q, k, oi, od) in enumerate(items):
         ai = torch.empty_like(oi)
         ad = torch.empty_like(od)
@@ -247,6 +271,9 @@ def run_batched(args, world, rank, local):
             err = float(np.max(np.abs(gd[ok] - rd[ok]) / np.maximum(np.abs(rd[ok]), 1e-30))) if ok.any() else 0.0
             recall_min = min(recall_min, rec)
             err_max = max(err_max, err)
+            if rec < 1.0:
+                recall_failures.append({"item": j, "nq": int(q.shape[0]), "k": k, "recall": rec, "max_rel_err": err,
+                                        "got": oi[:1, :3].cpu().tolist(), "ref": ri[:1, :3].tolist()})
 
     def timed(fn):
         for _ in range(args.warmup):
@@ -303,6 +330,7 @@ def run_batched(args, world, rank, local):
             "batch_speedup": ms_loop / ms_graph,
             "identical_to_alone": mismatches == 0, "items_differing": mismatches,
             "recall_at_k_min_sampled": recall_min, "max_rel_dist_err_sampled": err_max,
+            "recall_failures": recall_failures,
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": p_form, "unit": "TFLOP/s",
                          "frac": achieved / p_form, "traffic": None, "kernel": "whole graph (prep + fused + merge)",
                          "peak_kind": peak_kind + " bf16 burst", "algorithmic": "sum 2*nq*N*d"},
@@ -311,7 +339,7 @@ def run_batched(args, world, rank, local):
                     "h2d_bytes_per_step": sum(it[1].numel() * 4 for it in items),
                     "d2h_bytes_per_step": sum(it[3].numel() * 8 for it in items)},
             "gpu_launches": kernels * args.steps, "launches_per_step": {"graph": 1, "kernels_in_graph": kernels},
-            "workspace_bytes": ws_bytes,
+            "workspace_bytes": ws_bytes, "autotune": tuned,
             "clocks": sampler.summary(),
         }
         print(json.dumps(line), flush=True)
@@ -333,6 +361,7 @@ def main():
     ap.add_argument("--no-recall", action="store_true", help="skip the oracle recall check (profiling runs)")
     ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, "batched_uneven"])
     ap.add_argument("--batch-form", type=int, default=1, help="precision form of the batched workload")
+    ap.add_argument("--tune", action="store_true", help="batched workload: autotune its buckets first")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_init()
@@ -358,6 +387,7 @@ def main():
     dev = f"cuda:{local}"
     # every rank holds the same database and searches a full query batch (replicas)
     base, queries, k = synth.make(WORKLOAD, device=dev)
+    torch.cuda.synchronize()  # generated on torch's stream; the library orders its work on its own streams
     res = cb.DeviceResources(local)
     stream = torch.cuda.Stream(device=dev)
     Q = queries.shape[0]

@@ -106,6 +106,9 @@ def _load():
         "curplsh_batch_run": (i32, [vp, vp, i32]),
         "curplsh_batch_get_info": (i32, [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int64)]),
         "curplsh_batch_destroy": (i32, [vp]),
+        "curplsh_tuning_set": (i32, [i32, i32, i32, i64, i32, i32]),
+        "curplsh_tuning_get": (i32, [i32, i32, i32, i64, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+        "curplsh_tuning_clear": (i32, []),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -127,7 +130,8 @@ EXPORTED_SYMBOLS = (
     "curplsh_index_search_profiled", "curplsh_index_reset", "curplsh_index_get_dimension",
     "curplsh_index_get_num_data", "curplsh_index_get_device", "curplsh_compute_l2_norm",
     "curplsh_search_l2_distance", "curplsh_index_search_noalloc", "curplsh_batch_create", "curplsh_batch_run",
-    "curplsh_batch_get_info", "curplsh_batch_destroy",
+    "curplsh_batch_get_info", "curplsh_batch_destroy", "curplsh_tuning_set", "curplsh_tuning_get",
+    "curplsh_tuning_clear",
 )
 
 
@@ -417,3 +421,22 @@ class SearchBatch:
             self.close()
         except Exception:
             pass
+
+
+def tuning_set(precision: int, dim: int, k: int, num_queries: int, split_q4: int, pool_headroom: int) -> None:
+    """Sets the fused-pass parameters of one (precision, dim, k, Q) bucket (no reference counterpart)."""
+    _check(_lib.curplsh_tuning_set(int(precision), int(dim), int(k), int(num_queries), int(split_q4),
+                                   int(pool_headroom)))
+
+
+def tuning_get(precision: int, dim: int, k: int, num_queries: int):
+    """(split_q4, pool_headroom) of the bucket holding this shape."""
+    a = ctypes.c_int(0)
+    b = ctypes.c_int(0)
+    _check(_lib.curplsh_tuning_get(int(precision), int(dim), int(k), int(num_queries), ctypes.byref(a),
+                                   ctypes.byref(b)))
+    return a.value, b.value
+
+
+def tuning_clear() -> None:
+    _check(_lib.curplsh_tuning_clear())

@@ -69,7 +69,8 @@ bool is_device_ptr(const void* p, int dev) {
 
 struct FItem {
   int slot = 0;  // index (into Batch::uniq)
-  int form = 0, kp = 0, P = 0, d = 0;
+  int form = 0, kp = 0, P = 0, d = 0, k = 1;
+  TuneParams tune;
   int nq = 0;
   long long nq_pad = 0;
   std::vector<int> members;  // batch items, in order
@@ -112,6 +113,7 @@ struct curplsh_batch {
   uint32_t* host_status = nullptr;
   cudaStream_t cap = nullptr;
   cudaEvent_t fork = nullptr;
+  cudaEvent_t order_ev = nullptr;  // orders NULL-stream runs after the legacy default stream
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int kernels = 0;
@@ -175,8 +177,8 @@ int plan_batch(curplsh_batch* b) {
       x.slot = slot;
       x.form = form;
       x.kp = kp;
-      x.P = search_pool_capacity(kp);
       x.d = v.dim;
+      x.k = it.k;
       b->fitems.push_back(x);
     } else {
       fi = f->second;
@@ -187,6 +189,11 @@ int plan_batch(curplsh_batch* b) {
     x.members.push_back((int)i);
     x.row0.push_back(x.nq);
     x.nq += (int)it.num;
+  }
+  // tuned parameters per fused item, looked up with its concatenated query count
+  for (FItem& x : b->fitems) {
+    x.tune = tune_lookup(x.form, x.d, x.k, x.nq);
+    x.P = search_pool_capacity(x.kp, x.tune.headroom);
   }
   // ---- groups
   std::map<std::pair<int, int>, int> gmap;
@@ -244,10 +251,14 @@ int plan_batch(curplsh_batch* b) {
         const FItem& x = b->fitems[FL.fitems[j]];
         specs[j].nq = x.nq;
         specs[j].nb = (int)b->views[x.slot].n;
-        // units no longer than the item's own CTA ranges would be if it were
-        // searched alone, so its in-pool selection work stays what it is alone
+        // units as long as the item's own CTA ranges would be if it were
+        // searched alone (scaled by the tuned split), so its in-pool selection
+        // work stays what it is alone
         const long long own = (long long)((x.nq + kBM - 1) / kBM) * ((specs[j].nb + kBN - 1) / kBN);
-        specs[j].split_tiles = (int)std::max<long long>(1, (own + num_sms - 1) / num_sms);
+        // (clamped to the item's own range, as in a search alone, where a
+        // unit can never be longer than its CTA range)
+        specs[j].split_tiles = split_tiles_for(std::max<long long>(1, (own + num_sms - 1) / num_sms),
+                                               std::min(x.tune.split_q4, 4));
       }
       plan_fused_batch(specs.data(), (int)specs.size(), G.max_ctas, plans.data(), &FL.bp);
       for (size_t j = 0; j < FL.fitems.size(); ++j) {
@@ -549,6 +560,15 @@ int curplsh_batch_run(curplsh_batch* b, void* stream, int wait) {
     rc = plan_batch(b);
   }
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : b->views[0].stream;
+  if (!rc && !stream) {
+    cudaError_t e = b->order_ev ? cudaSuccess : cudaEventCreateWithFlags(&b->order_ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(b->order_ev, cudaStreamLegacy);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, b->order_ev, 0);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      rc = fail(CURPLSH_ERR_CUDA, "ordering after the legacy stream: %s", cudaGetErrorString(e));
+    }
+  }
   if (!rc) {
     cudaError_t e = cudaGraphLaunch(b->exec, st);
     if (e != cudaSuccess) {
@@ -589,6 +609,7 @@ int curplsh_batch_destroy(curplsh_batch* b) {
     b->drop_plan();
     if (b->cap) cudaStreamDestroy(b->cap);
     if (b->fork) cudaEventDestroy(b->fork);
+    if (b->order_ev) cudaEventDestroy(b->order_ev);
     if (b->host_status) cudaFreeHost(b->host_status);
   }
   delete b;

@@ -218,6 +218,7 @@ struct curplsh_index {
   float* xs = nullptr;            // [n_pad]
   uint32_t* status = nullptr;     // device error word
   long long generation = 0;       // bumped whenever the prepared database changes (add, reset)
+  cudaEvent_t order_ev = nullptr; // orders default-stream searches after the legacy stream
   std::map<cudaStream_t, std::unique_ptr<StreamWorkspace>> ws;
 
   void free_db() {
@@ -262,7 +263,9 @@ int kprime_for(int form, int k, int rerank_factor, int64_t n) {
 // refresh (warp radix select, cost ~ capacity) runs only when fewer than one
 // half tile of free slots remain, so each refresh absorbs >= max(k', 256)
 // survivors and refreshes stay rare.
-int pool_capacity(int kp) { return (int)round_up(kp + kHalfN + std::max(kp, 256), 32); }
+int pool_capacity(int kp, int headroom = kTuneDefaultHeadroom) {
+  return (int)round_up(kp + kHalfN + std::max(kp, headroom), 32);
+}
 
 struct Timing {
   cudaEvent_t ev[5] = {};
@@ -294,9 +297,10 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
     if (rc) return rc;
   }
   const int kp = kprime_for(form, k, rerank_factor, ix->n);
-  const int P = pool_capacity(kp);
+  const TuneParams tp = tune_lookup(form, d, k, nq);
+  const int P = pool_capacity(kp, tp.headroom);
   FusedPlan plan;
-  plan_fused(nq, (int)ix->n, ix->dres->num_sms, &plan);
+  plan_fused(nq, (int)ix->n, ix->dres->num_sms, &plan, tp.split_q4);
   const long long nq_pad = round_up(nq, kBM);
   const size_t pool_lists = (size_t)plan.num_qblocks * kBM * plan.units_per_block * 2;
 
@@ -400,9 +404,10 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
 size_t search_workspace_bytes(const curplsh_index* ix, int nq, int k, int form, int rerank_factor) {
   if (ix->n == 0) return 0;
   const int kp = kprime_for(form, k, rerank_factor, ix->n);
-  const int P = pool_capacity(kp);
+  const TuneParams tp = tune_lookup(form, ix->dim, k, nq);
+  const int P = pool_capacity(kp, tp.headroom);
   FusedPlan plan;
-  plan_fused(nq, (int)ix->n, ix->dres->num_sms, &plan);
+  plan_fused(nq, (int)ix->n, ix->dres->num_sms, &plan, tp.split_q4);
   const long long nq_pad = round_up(nq, kBM);
   const size_t pool_lists = (size_t)plan.num_qblocks * kBM * plan.units_per_block * 2;
   size_t b = 0;
@@ -432,6 +437,13 @@ int do_search(curplsh_index* ix, int64_t num, const float* queries, int k, int p
   std::lock_guard<std::mutex> lk(ix->mu);
   DeviceScope scope(ix->cfg.device);
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ix->dres->def;
+  if (!stream) {
+    // The resources' default stream is non-blocking; a search on it is ordered
+    // after the work already queued on the legacy default stream (where device
+    // queries are commonly produced), without blocking the host.
+    CUDA_TRY(cudaEventRecord(ix->order_ev, cudaStreamLegacy));
+    CUDA_TRY(cudaStreamWaitEvent(st, ix->order_ev, 0));
+  }
   const int nq = (int)num;
   const int dev = ix->cfg.device;
   const bool q_dev = pointer_device(queries) == dev;
@@ -543,7 +555,7 @@ int index_prepare_form(curplsh_index* ix, int form, IndexView* v) {
   return CURPLSH_OK;
 }
 int search_kprime(int form, int k, int rerank_factor, long long n) { return kprime_for(form, k, rerank_factor, n); }
-int search_pool_capacity(int kprime) { return pool_capacity(kprime); }
+int search_pool_capacity(int kprime, int headroom) { return pool_capacity(kprime, headroom); }
 int record_error(int code, const char* msg) { return set_error(code, "%s", msg); }
 }  // namespace curplsh_b200
 
@@ -684,6 +696,7 @@ int curplsh_index_bf_create(curplsh_resources* r, int dim, const curplsh_bf_conf
   DeviceScope scope(c.device);
   cudaError_t e = cudaMalloc(&ix->status, sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaMemset(ix->status, 0, sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ix->order_ev, cudaEventDisableTiming);
   if (e != cudaSuccess) {
     cudaGetLastError();
     delete ix;
@@ -706,6 +719,7 @@ int curplsh_index_destroy(curplsh_index* ix) {
     }
     ix->free_db();
     if (ix->status) cudaFree(ix->status);
+    if (ix->order_ev) cudaEventDestroy(ix->order_ev);
   }
   curplsh_resources* r = ix->res;
   delete ix;
@@ -734,6 +748,11 @@ int curplsh_index_add(curplsh_index* ix, int64_t num, const float* data) {
   const long long pad_new = round_up(n_new, kBN);
   const int src_dev = pointer_device(data);
   const bool borrow = ix->cfg.borrow_device_data && src_dev == ix->cfg.device && n_old == 0;
+  // Device rows are often produced just before add() by work on the legacy
+  // default stream (e.g. a framework's default stream), which the index's
+  // non-blocking stream does not wait for: wait for it here (add() is
+  // synchronous anyway).  Work on other streams must be complete already.
+  if (src_dev >= 0) CUDA_TRY(cudaStreamSynchronize(cudaStreamLegacy));
   // FP32 rows
   float* x32 = nullptr;
   if (borrow) {

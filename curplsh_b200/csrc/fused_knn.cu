@@ -862,18 +862,23 @@ void plan_fused_batch(const FusedItemSpec* specs, int n, int max_ctas, FusedItem
   }
 }
 
-void plan_fused(int nq, int nb, int num_sms, FusedPlan* out) {
+void plan_fused(int nq, int nb, int num_sms, FusedPlan* out, int split_q4) {
   FusedItemSpec s{};
   s.nq = nq;
   s.nb = nb;
   FusedItemPlan ip;
   FusedBatchPlan bp;
   plan_fused_batch(&s, 1, num_sms, &ip, &bp);
+  if (split_q4 < 4 && bp.grid > 0) {
+    s.split_tiles = split_tiles_for(bp.work_per_cta, split_q4);
+    plan_fused_batch(&s, 1, num_sms, &ip, &bp);
+  }
   out->num_qblocks = ip.num_qblocks;
   out->num_tiles = ip.num_tiles;
   out->work_per_cta = bp.work_per_cta;
   out->grid = bp.grid;
   out->units_per_block = ip.units_per_block;
+  out->split_tiles = ip.split_tiles;
 }
 
 uint32_t fused_smem_bytes(int form, int d) { return make_layout(form, d).total; }
@@ -944,7 +949,7 @@ cudaError_t launch_fused(const FusedLaunch& f, cudaStream_t st) {
   ip.num_qblocks = f.plan.num_qblocks;
   ip.num_tiles = f.plan.num_tiles;
   ip.units_per_block = f.plan.units_per_block;
-  ip.split_tiles = std::max(f.plan.num_tiles, 1);
+  ip.split_tiles = f.plan.split_tiles > 0 ? f.plan.split_tiles : std::max(f.plan.num_tiles, 1);
   ip.work_begin = 0;
   ip.work_end = (long long)f.plan.num_qblocks * f.plan.num_tiles;
   FusedBatchPlan bp;

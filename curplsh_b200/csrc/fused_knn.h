@@ -12,8 +12,24 @@ struct FusedPlan {
   int num_tiles = 0;          // T = ceil(nb / 256)
   long long work_per_cta = 0; // W
   int grid = 0;               // CTAs launched
-  int units_per_block = 0;    // U: max CTAs touching one query block
+  int units_per_block = 0;    // U: max units (pool lists) of one query block
+  int split_tiles = 1;        // L: resolved unit length limit
 };
+
+// Tuned launch parameters for one (form, d, k, Q) bucket (tuning.cpp).
+constexpr int kTuneDefaultHeadroom = 256;
+constexpr int kTuneMinHeadroom = 128;
+constexpr int kTuneMaxHeadroom = 8192;
+struct TuneParams {
+  int split_q4 = 4;                      // unit length limit in quarters of the search's own CTA range W
+  int headroom = kTuneDefaultHeadroom;   // pool capacity = k' + 128 + max(k', headroom), rounded to 32
+};
+TuneParams tune_lookup(int form, int d, int k, long long nq);
+// Unit length limit for an item whose own CTA range is w_own tiles (>= 1).
+inline int split_tiles_for(long long w_own, int split_q4) {
+  const long long s = (w_own * split_q4 + 3) / 4;
+  return (int)(s < 1 ? 1 : (s > (1LL << 30) ? (1LL << 30) : s));
+}
 
 struct FusedLaunch {
   int nq, nb, d, kprime, pool_cap, form;
@@ -40,7 +56,9 @@ struct FusedLaunch {
   FusedPlan plan;
 };
 
-void plan_fused(int nq, int nb, int num_sms, FusedPlan* out);
+// One search over at most num_sms CTAs.  split_q4 < 4 cuts units shorter than
+// the CTA ranges (split_tiles_for(W, split_q4)); >= 4 leaves the ranges whole.
+void plan_fused(int nq, int nb, int num_sms, FusedPlan* out, int split_q4 = 4);
 uint32_t fused_smem_bytes(int form, int d);
 cudaError_t launch_fused(const FusedLaunch& f, cudaStream_t st);
 
@@ -193,7 +211,7 @@ void index_unlock(curplsh_index* index);
 int index_prepare_form(curplsh_index* index, int form, IndexView* v);
 // Candidate count k' and pool capacity used by every search of this library.
 int search_kprime(int form, int k, int rerank_factor, long long n);
-int search_pool_capacity(int kprime);
+int search_pool_capacity(int kprime, int headroom = kTuneDefaultHeadroom);
 // Records a message for curplsh_last_error() and returns `code`.
 int record_error(int code, const char* msg);
 }  // namespace curplsh_b200

@@ -337,7 +337,7 @@ cudaError_t launch_merge_rerank(const MergeLaunch& m, cudaStream_t st) {
   it.num_tiles = m.plan.num_tiles;
   it.units_per_block = m.plan.units_per_block;
   it.row0 = 0;
-  it.split_tiles = m.plan.num_tiles > 0 ? m.plan.num_tiles : 1;
+  it.split_tiles = m.plan.split_tiles > 0 ? m.plan.split_tiles : 1;
   it.work_begin = 0;
   it.work_per_cta = m.plan.work_per_cta;
   it.pools = m.pools;

@@ -104,16 +104,19 @@ int curplsh_index_destroy(curplsh_index* index);
 int curplsh_index_train(curplsh_index* index, int64_t num, const float* data);
 /* Index::add (include/index.h:38, src/index_bf.cpp:26-44): rows get sequential labels; squared norms and
  * the quantised operand copies are computed once here.  Unlike the reference (one add only,
- * index_bf.cpp:27) further adds append. */
+ * index_bf.cpp:27) further adds append.  Synchronous; device `data` is read after the work already
+ * queued on the legacy default stream (work on other streams that writes it must be complete). */
 int curplsh_index_add(curplsh_index* index, int64_t num, const float* data);
 /* Index::search (include/index.h:52-53, src/index_bf.cpp:46-74): k nearest rows of every query,
  * ascending squared L2 distance, ties by lower row index; slots beyond the number of rows are
  * (-1, FLT_MAX).  k must be in [1, 1024] (search.cu:121-122).  Uses the index's default precision,
- * runs on the resources' default stream and returns when the results are in place. */
+ * runs on the resources' default stream (ordered after the work already queued on the legacy default
+ * stream) and returns when the results are in place. */
 int curplsh_index_search(curplsh_index* index, int64_t num, const float* queries, int k, int* indices,
                          float* distances);
 /* search with an explicit precision form (-1: index default), rerank factor (<= 0: index default)
- * and stream (NULL: default stream).  When queries, indices and distances are all device memory the
+ * and stream (NULL: the resources' default stream, ordered after the legacy default stream; an
+ * explicit stream is ordered only by itself).  When queries, indices and distances are all device memory the
  * call is asynchronous on `stream`; otherwise it synchronises before returning. */
 int curplsh_index_search_ex(curplsh_index* index, int64_t num, const float* queries, int k, int precision,
                             int rerank_factor, int* indices, float* distances, void* stream);
@@ -186,13 +189,29 @@ typedef struct curplsh_batch_item {
  * be called while the calling thread captures a stream. */
 int curplsh_batch_create(const curplsh_batch_item* items, int count, int precision, int rerank_factor,
                          curplsh_batch** out);
-/* Launches the graph on `stream` (NULL: the first index's default stream).  wait != 0 synchronises
+/* Launches the graph on `stream` (NULL: the first index's default stream, ordered after the work
+ * already queued on the legacy default stream).  wait != 0 synchronises
  * and checks the device status word.  An index changed by add()/reset() since the last plan is
  * re-planned (and the graph re-captured) first. */
 int curplsh_batch_run(curplsh_batch* batch, void* stream, int wait);
 /* Kernel launches in one run of the graph, and bytes of device working memory held. */
 int curplsh_batch_get_info(const curplsh_batch* batch, int* kernel_launches, int64_t* workspace_bytes);
 int curplsh_batch_destroy(curplsh_batch* batch);
+
+/* ------------------------------------------------------------ launch tuning */
+/* No counterpart in the reference (its tile sizes are fixed, src/internal/search.cu:12-77).  A
+ * process-wide table of fused-pass parameters per (precision, dim, k bucket, query-count bucket),
+ * buckets being ceil(log2 k) and floor(log2 num_queries).  Neither parameter changes any result:
+ *   split_q4       the longest run of database tiles one candidate pool covers, in quarters of
+ *                  the CTA range the search gets alone (4 = the range itself, the default;
+ *                  smaller values cut it; values above 4 act as 4);
+ *   pool_headroom  candidate-pool slack beyond k' + 128 keys (the k-select width; default 256).
+ * Filled by curplsh_b200.autotune, read by search, search_ex, search_profiled and the batch
+ * planner (the allocation-free search keeps the defaults). */
+int curplsh_tuning_set(int precision, int dim, int k, int64_t num_queries, int split_q4, int pool_headroom);
+/* Writes the bucket's parameters (the defaults when it was never set). */
+int curplsh_tuning_get(int precision, int dim, int k, int64_t num_queries, int* split_q4, int* pool_headroom);
+int curplsh_tuning_clear(void);
 
 #ifdef __cplusplus
 } /* extern "C" */

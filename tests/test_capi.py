@@ -87,3 +87,33 @@ def test_array_pointer_validation():
     with pytest.raises(TypeError):
         cb._ptr(np.zeros((4, 4), np.float32)[:, ::2], np.float32)
     assert cb._ptr(np.zeros((2, 2), np.float32), np.float32).value
+
+
+def test_tuning_table_roundtrip():
+    """The tuning table needs no GPU: set, bucketed get, defaults, clear, and argument checks."""
+    import curplsh_b200 as cb
+    cb.tuning_clear()
+    assert cb.tuning_get(1, 128, 100, 10000) == (4, 256)
+    cb.tuning_set(1, 128, 100, 10000, 2, 512)
+    # same bucket: k in (64, 128], nq in [8192, 16384)
+    assert cb.tuning_get(1, 128, 65, 8192) == (2, 512)
+    assert cb.tuning_get(1, 128, 128, 16383) == (2, 512)
+    # other buckets keep the defaults
+    assert cb.tuning_get(1, 128, 100, 16384) == (4, 256)
+    assert cb.tuning_get(0, 128, 100, 10000) == (4, 256)
+    assert cb.tuning_get(1, 64, 100, 10000) == (4, 256)
+    with pytest.raises(cb.CurplshError):
+        cb.tuning_set(1, 128, 100, 10000, 0, 512)
+    with pytest.raises(cb.CurplshError):
+        cb.tuning_set(1, 128, 100, 10000, 4, 64)
+    with pytest.raises(cb.CurplshError):
+        cb.tuning_set(3, 128, 100, 10000, 4, 256)
+    cb.tuning_clear()
+    assert cb.tuning_get(1, 128, 100, 10000) == (4, 256)
+
+
+def test_autotune_bucket_matches_library():
+    from curplsh_b200 import autotune
+    assert autotune.bucket(1, 128, 100, 10000) == "1,128,7,13"
+    assert autotune.bucket(0, 64, 1, 1) == "0,64,0,0"
+    assert autotune.bucket(2, 96, 1024, 4096) == "2,96,10,12"
