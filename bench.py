@@ -351,6 +351,127 @@ def run_batched(args, world, rank, local):
     return 0
 
 
+def run_serving(args, world, rank, local):
+    """--workload serving: one resident database (N = 5,000,000, d = 256,
+    BF16-valued Gaussian mixture of 2,048 centroids), requests of 1-256
+    queries (log-uniform) arriving as a Poisson process, k = 50, queries and
+    results in pinned host memory.  For the BF16 + rerank form and the plain
+    FP32-exact form: saturated throughput (every request queued at once) and,
+    per offered rate, p50 / p99 latency (submit to results in host memory)
+    and achieved throughput."""
+    import numpy as np
+    import torch
+
+    import curplsh_b200 as cb
+    import oracle
+    from curplsh_b200 import synth
+
+    torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
+    n, d, k = args.serve_n, 256, 50
+    base, qpool = synth.mixture_bf16(n, 20000, d, device=dev)
+    torch.cuda.synchronize()
+    res = cb.DeviceResources(local)
+    ix = cb.IndexBF(res, d, cb.IndexBFConfig(device=local, precision=1))
+    ix.add(n, base)
+    qpool_h = qpool.cpu().pin_memory()
+    rng = np.random.default_rng(17 + rank)
+
+    def request_sizes(count):
+        return [int(round(np.exp(rng.uniform(0.0, np.log(256))))) for _ in range(count)]
+
+    def make_outputs(sizes):
+        return [(torch.empty((m, k), dtype=torch.int32).pin_memory(), torch.empty((m, k)).pin_memory())
+                for m in sizes]
+
+    def run_load(srv, sizes, arrivals):
+        """Submits request i at arrivals[i] seconds; returns (latencies, wall seconds, results)."""
+        outs = make_outputs(sizes)
+        offs = np.cumsum([0] + sizes[:-1]) % (qpool_h.shape[0] - 256)
+        qs = [qpool_h[o:o + m] for o, m in zip(offs, sizes)]
+        tickets = [None] * len(sizes)
+        lat = [None] * len(sizes)
+        done = threading.Event()
+
+        def waiter():
+            for i in range(len(sizes)):
+                while tickets[i] is None:
+                    time.sleep(20e-6)
+                lat[i] = srv.wait(tickets[i], timeout=600.0)
+            done.set()
+
+        th = threading.Thread(target=waiter)
+        th.start()
+        t0 = time.perf_counter()
+        for i, m in enumerate(sizes):
+            due = t0 + arrivals[i]
+            while True:
+                now = time.perf_counter()
+                if now >= due:
+                    break
+                time.sleep(min(due - now, 500e-6))
+            tickets[i] = srv.submit(qs[i], k, outs[i][0], outs[i][1])
+        done.wait()
+        wall = time.perf_counter() - t0
+        th.join()
+        return np.array(lat), wall, (qs, outs)
+
+    forms_out = {}
+    recall = None
+    for form in (1, 0):
+        srv = cb.Server(ix, precision=form, max_inflight=3, max_step_queries=4096, memory_budget=4 << 30)
+        # warm-up
+        sizes = request_sizes(64)
+        run_load(srv, sizes, [0.0] * len(sizes))
+        # saturated throughput: every request queued at once
+        sizes = request_sizes(600)
+        lat, wall, (qs, outs) = run_load(srv, sizes, [0.0] * len(sizes))
+        sat = sum(sizes) / wall
+        if form == 1:
+            # a sample of served results, checked against the FP64 oracle after all timing
+            qsample = np.concatenate([qs[i][:1].numpy() for i in range(8)])
+            gsample = np.concatenate([outs[i][0][:1].numpy() for i in range(8)])
+        per_rate = {}
+        for rate in args.serve_rates:
+            mean_req = rate / 46.0  # mean of the log-uniform 1..256 request size is ~46 queries
+            count = int(min(3000, max(200, mean_req * args.serve_seconds)))
+            sizes = request_sizes(count)
+            gaps = rng.exponential(1.0 / mean_req, size=count)
+            arrivals = np.cumsum(gaps) - gaps[0]
+            lat, wall, _ = run_load(srv, sizes, list(arrivals))
+            per_rate[str(rate)] = {"p50_ms": float(np.percentile(lat, 50) * 1e3),
+                                   "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                                   "achieved_queries_per_s": sum(sizes) / wall, "requests": count}
+        st = srv.stats()
+        srv.close()
+        forms_out[FORMS[form]] = {"saturated_queries_per_s": sat, "rates": per_rate,
+                                  "steps": st["steps"], "max_inflight_seen": st["max_inflight_seen"],
+                                  "peak_bytes_in_use": st["peak_bytes_in_use"],
+                                  "kernel_launches": st["kernel_launches"]}
+    if rank == 0 and not args.no_recall:
+        base_h = base.cpu().numpy()
+        rd, ri = oracle.knn(base_h, qsample, k)
+        recall, _ = oracle.recall_at_k(base_h, qsample, gsample, rd)
+    if rank == 0:
+        b = forms_out["bf16_rerank"]
+        line = {
+            "metric": "serving p50/p99 latency (ms) and queries/s", "value": b["saturated_queries_per_s"],
+            "unit": "queries/s", "n_gpus": world, "steps": None, "warmup": 1, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
+            "data": "synthetic (seeded Gaussian mixture, 2048 centroids, BF16-valued)",
+            "config": {"workload": "serving", "N": n, "d": d, "k": k, "request_queries": "log-uniform 1-256",
+                       "arrivals": "Poisson", "io": "pinned host queries and results",
+                       "max_inflight": 3, "memory_budget_bytes": 4 << 30},
+            "recall_at_k_sampled": recall, "forms": forms_out,
+            "bf16_vs_exact_saturated": b["saturated_queries_per_s"] / forms_out["fp32_exact"]["saturated_queries_per_s"],
+        }
+        print(json.dumps(line), flush=True)
+    ix.close()
+    res.close()
+    barrier(world)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -359,7 +480,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--forms", default="0,1,2", help="precision forms to time (0 exact, 1 bf16, 2 fp8)")
     ap.add_argument("--no-recall", action="store_true", help="skip the oracle recall check (profiling runs)")
-    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, "batched_uneven"])
+    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, "batched_uneven", "serving"])
+    ap.add_argument("--serve-n", type=int, default=5_000_000, help="serving workload: database rows")
+    ap.add_argument("--serve-rates", type=lambda v: [int(x) for x in v.split(",")], default=[1000, 5000, 20000, 50000],
+                    help="serving workload: offered query rates (queries/s)")
+    ap.add_argument("--serve-seconds", type=float, default=3.0, help="serving workload: seconds per rate")
     ap.add_argument("--batch-form", type=int, default=1, help="precision form of the batched workload")
     ap.add_argument("--tune", action="store_true", help="batched workload: autotune its buckets first")
     args = ap.parse_args()
@@ -369,8 +494,8 @@ def main():
         rc = run_reference(args, world, rank)
         barrier(world)
         return rc
-    if args.workload == "batched_uneven":
-        rc = run_batched(args, world, rank, local)
+    if args.workload in ("batched_uneven", "serving"):
+        rc = (run_batched if args.workload == "batched_uneven" else run_serving)(args, world, rank, local)
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()

@@ -22,7 +22,7 @@ import numpy as np
 
 __all__ = [
     "DeviceResources", "IndexBF", "IndexBFConfig", "MemorySpace", "Precision", "CurplshError",
-    "compute_l2_norm", "search_l2_distance", "lib_path", "get_num_devices", "SearchBatch",
+    "compute_l2_norm", "search_l2_distance", "lib_path", "get_num_devices", "SearchBatch", "Server",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -62,6 +62,19 @@ class _BatchItem(ctypes.Structure):
     _fields_ = [("index", ctypes.c_void_p), ("num", ctypes.c_int64), ("queries", ctypes.c_void_p),
                 ("k", ctypes.c_int32), ("pad0", ctypes.c_int32), ("indices", ctypes.c_void_p),
                 ("distances", ctypes.c_void_p)]
+
+
+class _ServerCfg(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int32), ("rerank_factor", ctypes.c_int32),
+                ("max_inflight", ctypes.c_int32), ("max_step_queries", ctypes.c_int32),
+                ("memory_budget", ctypes.c_int64)]
+
+
+class _ServerStats(ctypes.Structure):
+    _fields_ = [("requests_done", ctypes.c_int64), ("queries_done", ctypes.c_int64), ("steps", ctypes.c_int64),
+                ("kernel_launches", ctypes.c_int64), ("max_step_queries", ctypes.c_int64),
+                ("peak_bytes_in_use", ctypes.c_int64), ("max_inflight_seen", ctypes.c_int32),
+                ("pad0", ctypes.c_int32), ("busy_seconds", ctypes.c_double)]
 
 
 def lib_path() -> str:
@@ -109,6 +122,12 @@ def _load():
         "curplsh_tuning_set": (i32, [i32, i32, i32, i64, i32, i32]),
         "curplsh_tuning_get": (i32, [i32, i32, i32, i64, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
         "curplsh_tuning_clear": (i32, []),
+        "curplsh_server_config_init": (None, [ctypes.POINTER(_ServerCfg)]),
+        "curplsh_server_create": (i32, [vp, ctypes.POINTER(_ServerCfg), ctypes.POINTER(vp)]),
+        "curplsh_server_submit": (i32, [vp, i64, f32p, i32, i32p, f32p, ctypes.POINTER(ctypes.c_int64)]),
+        "curplsh_server_wait": (i32, [vp, i64, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]),
+        "curplsh_server_get_stats": (i32, [vp, ctypes.POINTER(_ServerStats)]),
+        "curplsh_server_destroy": (i32, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -131,7 +150,8 @@ EXPORTED_SYMBOLS = (
     "curplsh_index_get_num_data", "curplsh_index_get_device", "curplsh_compute_l2_norm",
     "curplsh_search_l2_distance", "curplsh_index_search_noalloc", "curplsh_batch_create", "curplsh_batch_run",
     "curplsh_batch_get_info", "curplsh_batch_destroy", "curplsh_tuning_set", "curplsh_tuning_get",
-    "curplsh_tuning_clear",
+    "curplsh_tuning_clear", "curplsh_server_config_init", "curplsh_server_create", "curplsh_server_submit",
+    "curplsh_server_wait", "curplsh_server_get_stats", "curplsh_server_destroy",
 )
 
 
@@ -440,3 +460,59 @@ def tuning_get(precision: int, dim: int, k: int, num_queries: int):
 
 def tuning_clear() -> None:
     _check(_lib.curplsh_tuning_clear())
+
+
+class Server:
+    """Serving loop with continuous batching over one resident index (no
+    counterpart in the reference).  ``submit`` queues a request and returns a
+    ticket at once; ``wait`` blocks until its results are written and returns
+    the request's latency in seconds.  Arrays may be host (numpy / CPU torch)
+    or CUDA tensors; they must stay alive and unmodified until ``wait``."""
+
+    def __init__(self, index: "IndexBF", precision: int = -1, rerank_factor: int = 0, max_inflight: int = 3,
+                 max_step_queries: int = 4096, memory_budget: int = 2 << 30):
+        cfg = _ServerCfg()
+        _lib.curplsh_server_config_init(ctypes.byref(cfg))
+        cfg.precision = int(precision)
+        cfg.rerank_factor = int(rerank_factor)
+        cfg.max_inflight = int(max_inflight)
+        cfg.max_step_queries = int(max_step_queries)
+        cfg.memory_budget = int(memory_budget)
+        h = ctypes.c_void_p()
+        _check(_lib.curplsh_server_create(index._h, ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self._index = index
+        self._keep = {}
+
+    def submit(self, queries, k: int, indices, distances) -> int:
+        t = ctypes.c_int64(0)
+        _check(_lib.curplsh_server_submit(self._h, int(queries.shape[0]), _ptr(queries, np.float32), int(k),
+                                          _ptr(indices, np.int32, True), _ptr(distances, np.float32, True),
+                                          ctypes.byref(t)))
+        self._keep[t.value] = (queries, indices, distances)
+        return t.value
+
+    def wait(self, ticket: int, timeout: float = -1.0) -> float:
+        lat = ctypes.c_double(0.0)
+        rc = _lib.curplsh_server_wait(self._h, int(ticket), float(timeout), ctypes.byref(lat))
+        if rc != ERR_STATE:  # anything but a time-out ends the ticket
+            self._keep.pop(ticket, None)
+        _check(rc)
+        return lat.value
+
+    def stats(self) -> dict:
+        st = _ServerStats()
+        _check(_lib.curplsh_server_get_stats(self._h, ctypes.byref(st)))
+        return {name: getattr(st, name) for name, _ in _ServerStats._fields_ if name != "pad0"}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.curplsh_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -105,6 +105,26 @@ def normal_bf16(rows: int, d: int, seed: int, device="cuda", chunk: int = 1 << 2
     return out
 
 
+def mixture_bf16(n: int, q: int, d: int = 256, centroids: int = 2048, sigma: float = 0.25, seed: int = 4,
+                 device="cuda", chunk: int = 1 << 20):
+    """Gaussian mixture with N(0,1) centroids and per-point N(0, sigma^2)
+    offsets, values rounded to BF16 and stored FP32.  Queries come from the
+    same mixture."""
+    g = _gen(device, seed)
+    cent = torch.randn((centroids, d), generator=g, device=device)
+
+    def draw(m):
+        out = torch.empty((m, d), device=device)
+        for s in range(0, m, chunk):
+            e = min(m, s + chunk)
+            lab = torch.randint(0, centroids, (e - s,), generator=g, device=device)
+            x = cent[lab] + sigma * torch.randn((e - s, d), generator=g, device=device)
+            out[s:e] = x.bfloat16().float()
+        return out
+
+    return draw(n), draw(q)
+
+
 def make(name: str, device="cuda", n: int | None = None, q: int | None = None):
     """Inputs of a named configuration (optionally with N or Q overridden)."""
     N, Q, d, k = CONFIGS[name]

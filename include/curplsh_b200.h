@@ -198,6 +198,54 @@ int curplsh_batch_run(curplsh_batch* batch, void* stream, int wait);
 int curplsh_batch_get_info(const curplsh_batch* batch, int* kernel_launches, int64_t* workspace_bytes);
 int curplsh_batch_destroy(curplsh_batch* batch);
 
+/* ------------------------------------------------------------ serving loop */
+/* No counterpart in the reference.  Continuous batching of search requests against one resident
+ * index: curplsh_server_submit() queues a request and returns a ticket at once; a scheduler thread
+ * forms steps from the waiting requests (first come, first served, at most max_step_queries queries)
+ * and issues each step -- prep, fused filter, merge + rerank -- on one of max_inflight streams, so
+ * requests that arrive while earlier steps run are admitted and run concurrently with them.
+ * Admission is by device memory: all in-flight steps share one arena of memory_budget bytes
+ * allocated at creation, and a step waits until its working memory fits.  Every result equals
+ * curplsh_index_search_ex of that request alone with the server's precision and rerank factor.
+ * queries, indices and distances may be host or device memory (device memory of the index's
+ * device); they must stay valid, and unmodified, until curplsh_server_wait() returns for the
+ * ticket.  Changing the index (add, reset) while requests are in flight is not supported. */
+typedef struct curplsh_server curplsh_server;
+
+typedef struct curplsh_server_config {
+  int32_t precision;        /* -1 (default): the index's default precision */
+  int32_t rerank_factor;    /* <= 0 (default): the index's */
+  int32_t max_inflight;     /* steps on the GPU at once (default 3, at most 16) */
+  int32_t max_step_queries; /* queries per step and per request (default 4096) */
+  int64_t memory_budget;    /* device bytes for all in-flight steps (default 2 GiB) */
+} curplsh_server_config;
+
+typedef struct curplsh_server_stats {
+  int64_t requests_done;
+  int64_t queries_done;
+  int64_t steps;
+  int64_t kernel_launches;    /* kernels issued by all steps */
+  int64_t max_step_queries;   /* largest step formed */
+  int64_t peak_bytes_in_use;  /* largest arena use */
+  int32_t max_inflight_seen;  /* most steps on the GPU at once */
+  int32_t pad0;
+  double busy_seconds;        /* wall time with at least one step on the GPU */
+} curplsh_server_stats;
+
+void curplsh_server_config_init(curplsh_server_config* cfg);
+int curplsh_server_create(curplsh_index* index, const curplsh_server_config* cfg, curplsh_server** out);
+/* Queues num (1..max_step_queries) queries; rejects requests whose working memory alone exceeds the
+ * budget. */
+int curplsh_server_submit(curplsh_server* server, int64_t num, const float* queries, int k, int32_t* indices,
+                          float* distances, int64_t* ticket);
+/* Waits for a ticket (timeout_s < 0: no limit; CURPLSH_ERR_STATE on time-out, the ticket stays valid),
+ * returns its status and, when latency_s is not NULL, seconds from submit to completion.  A ticket
+ * can be waited for once. */
+int curplsh_server_wait(curplsh_server* server, int64_t ticket, double timeout_s, double* latency_s);
+int curplsh_server_get_stats(curplsh_server* server, curplsh_server_stats* out);
+/* Finishes every queued request, then frees the server. */
+int curplsh_server_destroy(curplsh_server* server);
+
 /* ------------------------------------------------------------ launch tuning */
 /* No counterpart in the reference (its tile sizes are fixed, src/internal/search.cu:12-77).  A
  * process-wide table of fused-pass parameters per (precision, dim, k bucket, query-count bucket),
