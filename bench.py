@@ -6,6 +6,12 @@ queries, d = 128, k = 100, integer-valued FP32 data from 1,000 centroids
 (seeded synthetic data, see curplsh_b200/synth.py).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload mixture_int_1m|sphere_10m|batched_uneven|serving]
+
+Other workloads: sphere_10m (N = 10,000,000, Q = 10,000, d = 96, k = 10,
+unit-sphere mixture, FP8-E4M3 + rerank headline), batched_uneven (64 query
+batches over 8 databases in one graph replay) and serving (continuous batching
+of Poisson-arriving requests; p50/p99 latency and throughput).
 
 Prints ONE JSON line (rank 0).  `value` is queries/s of the headline form
 (BF16 coarse + exact FP32 rerank) with queries resident in HBM, kernels timed
@@ -33,11 +39,18 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD = "mixture_int_1m"
-N_DB, N_Q, DIM, K = 1_000_000, 10_000, 128, 100
 FORMS = {0: "fp32_exact", 1: "bf16_rerank", 2: "fp8_rerank"}
-HEADLINE_FORM = 1
 RECALL_SAMPLE = 128       # queries checked against the oracle per form
 METRIC = "queries/s at recall@k=1.0"
+# single-search workloads: headline form, forms timed by default, data description
+WORKLOADS = {
+    "mixture_int_1m": {"headline": 1, "forms": "0,1,2",
+                       "data": "synthetic (seeded Gaussian mixture, 1000 centroids, sigma 12, integer-valued FP32)",
+                       "l2": "database (1.0 GB FP32 + 0.5 GB BF16 copies) larger than L2"},
+    "sphere_10m": {"headline": 2, "forms": "0,2",
+                   "data": "synthetic (seeded Gaussian mixture on the unit sphere, 4096 centroids, sigma 0.05)",
+                   "l2": "database (3.8 GB FP32, 1.0 GB FP8 copy) larger than L2"},
+}
 
 
 def load_peaks():
@@ -49,14 +62,14 @@ def load_peaks():
     return 6650.0, 1590.0, 1400.0, "fallback"
 
 
-def load_traffic(form_name):
+def load_traffic(workload, form_name):
     """DRAM bytes per fused launch from the committed ncu summary, if any."""
     p = os.path.join(ROOT, "profiles", "fused_knn_traffic.json")
     if not os.path.exists(p):
         return None
     with open(p) as f:
         d = json.load(f)
-    return d.get(WORKLOAD, {}).get(form_name)
+    return d.get(workload, {}).get(form_name)
 
 
 class ClockSampler:
@@ -161,7 +174,9 @@ def run_reference(args, world, rank):
     import oracle
     from curplsh_b200 import synth
     dev = "cuda" if torch.cuda.is_available() else "cpu"
-    base, queries, k = synth.make(WORKLOAD, device=dev)
+    wl = args.workload if args.workload in WORKLOADS else WORKLOAD
+    n_db, n_q, dim, _ = synth.CONFIGS[wl]
+    base, queries, k = synth.make(wl, device=dev)
     base_h = base.cpu().numpy()
     q_h = queries.cpu().numpy()
     sample = 128
@@ -179,10 +194,10 @@ def run_reference(args, world, rank):
     line = {
         "impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian mixture, integer-valued)",
-        "config": {"workload": WORKLOAD, "N": N_DB, "Q": N_Q, "d": DIM, "k": K, "q_per_step_sample": sample},
+        "vs_baseline": None, "dtype": "f64", "data": WORKLOADS[wl]["data"],
+        "config": {"workload": wl, "N": n_db, "Q": n_q, "d": dim, "k": k, "q_per_step_sample": sample},
         "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": cores, "kind": "port",
-                         "sample": f"{sample} queries per step against all {N_DB} rows"},
+                         "sample": f"{sample} queries per step against all {n_db} rows"},
         "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference ships no CPU search; this arm times the FP64 restatement of its searchL2Distance "
                 "semantics (oracle/knn_oracle.c) on the host cores",
@@ -478,9 +493,9 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--forms", default="0,1,2", help="precision forms to time (0 exact, 1 bf16, 2 fp8)")
+    ap.add_argument("--forms", default=None, help="precision forms to time (0 exact, 1 bf16, 2 fp8)")
     ap.add_argument("--no-recall", action="store_true", help="skip the oracle recall check (profiling runs)")
-    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, "batched_uneven", "serving"])
+    ap.add_argument("--workload", default=WORKLOAD, choices=list(WORKLOADS) + ["batched_uneven", "serving"])
     ap.add_argument("--serve-n", type=int, default=5_000_000, help="serving workload: database rows")
     ap.add_argument("--serve-rates", type=lambda v: [int(x) for x in v.split(",")], default=[1000, 5000, 20000, 50000],
                     help="serving workload: offered query rates (queries/s)")
@@ -510,8 +525,11 @@ def main():
 
     torch.cuda.set_device(local)
     dev = f"cuda:{local}"
+    wl = args.workload
+    info = WORKLOADS[wl]
+    n_db, _, dim, _ = synth.CONFIGS[wl]
     # every rank holds the same database and searches a full query batch (replicas)
-    base, queries, k = synth.make(WORKLOAD, device=dev)
+    base, queries, k = synth.make(wl, device=dev)
     torch.cuda.synchronize()  # generated on torch's stream; the library orders its work on its own streams
     res = cb.DeviceResources(local)
     stream = torch.cuda.Stream(device=dev)
@@ -528,13 +546,13 @@ def main():
         qs_h = queries[sub].cpu().numpy()
         rate, rd, ri, cores = cpu_oracle_rate(base_h, qs_h, k, RECALL_SAMPLE)
         cpu = {"value": rate, "unit": "queries/s", "cores": cores, "kind": "port",
-               "sample": f"{RECALL_SAMPLE} queries against all {N_DB} rows (FP64 oracle, OpenMP)"}
-    forms = [int(f) for f in args.forms.split(",") if f != ""]
-    headline = HEADLINE_FORM if HEADLINE_FORM in forms else forms[0]
+               "sample": f"{RECALL_SAMPLE} queries against all {n_db} rows (FP64 oracle, OpenMP)"}
+    forms = [int(f) for f in (args.forms or info["forms"]).split(",") if f != ""]
+    headline = info["headline"] if info["headline"] in forms else forms[0]
     indexes = {}
     for form in forms:
-        ix = cb.IndexBF(res, DIM, cb.IndexBFConfig(device=local, precision=form))
-        ix.add(N_DB, base)
+        ix = cb.IndexBF(res, dim, cb.IndexBFConfig(device=local, precision=form))
+        ix.add(n_db, base)
         indexes[form] = ix
         ix.search_ex(Q, queries, k, oi, od, stream=stream)
         stream.synchronize()
@@ -547,7 +565,7 @@ def main():
 
     # ---- timed region: device-resident queries, CUDA events on our stream
     peaks = load_peaks()
-    flops = 2.0 * Q * N_DB * DIM
+    flops = 2.0 * Q * n_db * dim
     launches_per_step = 3  # query prep, fused tensor-core filter, merge + rerank
     timing = {}
     clocks = None
@@ -579,7 +597,7 @@ def main():
         timing[form] = (ms, fused_ms, passes)
 
     # ---- end to end through the C ABI: pinned host queries in, host results out
-    qh = torch.empty((Q, DIM), dtype=torch.float32, pin_memory=True)
+    qh = torch.empty((Q, dim), dtype=torch.float32, pin_memory=True)
     qh.copy_(queries.cpu())
     ih = torch.empty((Q, k), dtype=torch.int32, pin_memory=True)
     dh = torch.empty((Q, k), dtype=torch.float32, pin_memory=True)
@@ -613,20 +631,20 @@ def main():
         line = {
             "metric": METRIC, "value": Q * world / (ms / 1e3), "unit": "queries/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
-            "data": "synthetic (seeded Gaussian mixture, 1000 centroids, sigma 12, integer-valued FP32)",
-            "config": {"workload": WORKLOAD, "N": N_DB, "Q": Q, "d": DIM, "k": k, "form": FORMS[headline],
-                       "rerank_factor": 4, "l2": "database (1.0 GB FP32 + 0.5 GB BF16 copies) larger than L2",
+            "scaling": "weak", "vs_baseline": None, "dtype": FORMS[headline].split("_")[0],
+            "data": info["data"],
+            "config": {"workload": wl, "N": n_db, "Q": Q, "d": dim, "k": k, "form": FORMS[headline],
+                       "rerank_factor": 4, "l2": info["l2"],
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "recall_at_k": rec, "recall_ok": rec_ok,
             "forms": forms_out,
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": bf16_burst, "unit": "TFLOP/s",
-                         "frac": achieved / bf16_burst, "traffic": load_traffic(FORMS[headline]),
+                         "frac": achieved / bf16_burst, "traffic": load_traffic(wl, FORMS[headline]),
                          "kernel": f"fused_knn_kernel<{FORMS[headline]}>", "peak_kind": peak_kind + " bf16 burst",
                          "algorithmic": "2*Q*N*d flops per launch"},
             "cpu_baseline": cpu,
             "e2e": {"value": Q * world / (e2e / 1e3), "unit": "queries/s", "ms_per_step": e2e,
-                    "h2d_bytes_per_step": Q * DIM * 4, "d2h_bytes_per_step": Q * k * 8},
+                    "h2d_bytes_per_step": Q * dim * 4, "d2h_bytes_per_step": Q * k * 8},
             "gpu_launches": launches_per_step * args.steps,
             "launches_per_step": {"prep_rows_kernel": 1, "fused_knn_kernel": 1, "merge_rerank_kernel": 1},
             "clocks": clocks,

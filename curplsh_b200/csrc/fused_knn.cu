@@ -558,6 +558,18 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
             nb_h1 = ld_relaxed_u32(&qbh[1]);
           }
         }
+        // FP8: this half tile's database norms and scales, loaded before the
+        // accumulator wait (their latency overlaps it) and staged in the
+        // warp's histogram area, which is free outside a refresh
+        float pxn[4], psx[4];
+        if (Tr::kFP8) {
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const int c = t * kBN + g * kHalfN + lane + 32 * i;  // < nb_pad: rows are padded to whole tiles
+            pxn[i] = __ldg(p.db_norms + c);
+            psx[i] = __ldg(p.db_scale + c);
+          }
+        }
         STAT_BEGIN(tw);
         if (!wait_or_abort(&acc_full[slot], use & 1u, abort_flag)) {
           raise_abort(abort_flag, B.status, kErrWaitTimeout);
@@ -568,6 +580,16 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
         STAT_BEGIN(tfl);
         tc_fence_after();
         const int colh = t * kBN + g * kHalfN;
+        float* colv = reinterpret_cast<float*>(hist);  // [128] norms, then [128] scales
+        if (Tr::kFP8) {
+          __syncwarp();
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            colv[lane + 32 * i] = pxn[i];
+            colv[kHalfN + lane + 32 * i] = psx[i];
+          }
+          __syncwarp();
+        }
 #pragma unroll 1
         for (int h = 0; h < kHalfN / 64; ++h) {
           uint32_t v[64];
@@ -586,12 +608,12 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
               db[j] = __uint_as_float(v[32 + j]);
             }
           } else {
-            const float4* xn4 = reinterpret_cast<const float4*>(p.db_norms + col0);
-            const float4* sx4 = reinterpret_cast<const float4*>(p.db_scale + col0);
+            const float4* xn4 = reinterpret_cast<const float4*>(colv + h * 64);
+            const float4* sx4 = reinterpret_cast<const float4*>(colv + kHalfN + h * 64);
 #pragma unroll
             for (int j4 = 0; j4 < 16; ++j4) {
-              const float4 xn = __ldg(xn4 + j4);
-              const float4 sx = __ldg(sx4 + j4);
+              const float4 xn = xn4[j4];
+              const float4 sx = sx4[j4];
               float* dst = j4 < 8 ? da : db;
               const int o = (j4 & 7) * 4;
               dst[o + 0] = fmaf(__uint_as_float(v[4 * j4 + 0]) * sx.x, m2s, xn.x);
