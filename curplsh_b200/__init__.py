@@ -128,6 +128,7 @@ def _load():
         "curplsh_server_wait": (i32, [vp, i64, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]),
         "curplsh_server_get_stats": (i32, [vp, ctypes.POINTER(_ServerStats)]),
         "curplsh_server_destroy": (i32, [vp]),
+        "curplsh_merge_shard_results": (i32, [i64, i32, i32, f32p, i32p, vp, i32p, f32p, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -151,7 +152,7 @@ EXPORTED_SYMBOLS = (
     "curplsh_search_l2_distance", "curplsh_index_search_noalloc", "curplsh_batch_create", "curplsh_batch_run",
     "curplsh_batch_get_info", "curplsh_batch_destroy", "curplsh_tuning_set", "curplsh_tuning_get",
     "curplsh_tuning_clear", "curplsh_server_config_init", "curplsh_server_create", "curplsh_server_submit",
-    "curplsh_server_wait", "curplsh_server_get_stats", "curplsh_server_destroy",
+    "curplsh_server_wait", "curplsh_server_get_stats", "curplsh_server_destroy", "curplsh_merge_shard_results",
 )
 
 
@@ -516,3 +517,16 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def merge_shard_results(distances, indices, shard_bases, out_indices, out_distances, stream=None) -> None:
+    """Global top-k from per-shard results (CUDA tensors): distances [G, Q, k] float32, indices
+    [G, Q, k] int32 (shard-local rows), shard_bases [G] int64 (first global row of each shard)."""
+    import torch
+    if shard_bases.dtype != torch.int64 or not shard_bases.is_contiguous():
+        raise TypeError("shard_bases must be a contiguous int64 tensor")
+    G, Q, k = (int(x) for x in distances.shape)
+    _check(_lib.curplsh_merge_shard_results(Q, k, G, _ptr(distances, np.float32), _ptr(indices, np.int32),
+                                            ctypes.c_void_p(shard_bases.data_ptr()),
+                                            _ptr(out_indices, np.int32, True), _ptr(out_distances, np.float32, True),
+                                            _stream_ptr(stream)))

@@ -246,6 +246,17 @@ int curplsh_server_get_stats(curplsh_server* server, curplsh_server_stats* out);
 /* Finishes every queued request, then frees the server. */
 int curplsh_server_destroy(curplsh_server* server);
 
+/* ------------------------------------------------------------ sharded search */
+/* No counterpart in the reference (one device per index, include/index.h:18-82).  Merges the top-k
+ * lists of a database split by rows over num_shards shards: distances and indices are device arrays
+ * [num_shards][num_queries][k] (each shard's search result with shard-local row indices, as an
+ * all-gather lays them out), shard_bases a device array [num_shards] of each shard's first global
+ * row.  Writes the global top-k, ascending distance, ties by lower global row, padding (-1,
+ * FLT_MAX).  Asynchronous on `stream`; num_shards * k <= 16384. */
+int curplsh_merge_shard_results(int64_t num_queries, int k, int num_shards, const float* distances,
+                                const int32_t* indices, const int64_t* shard_bases, int32_t* out_indices,
+                                float* out_distances, void* stream);
+
 /* ------------------------------------------------------------ launch tuning */
 /* No counterpart in the reference (its tile sizes are fixed, src/internal/search.cu:12-77).  A
  * process-wide table of fused-pass parameters per (precision, dim, k bucket, query-count bucket),
