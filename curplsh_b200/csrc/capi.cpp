@@ -259,12 +259,19 @@ int kprime_for(int form, int k, int rerank_factor, int64_t n) {
   return (int)kp;
 }
 
-// Pool capacity: k' kept keys + room for one half tile + refresh headroom.  A
-// refresh (warp radix select, cost ~ capacity) runs only when fewer than one
-// half tile of free slots remain, so each refresh absorbs >= max(k', 256)
-// survivors and refreshes stay rare.
+// Pool capacity: k' kept keys + room for one tile (both halves append to the
+// pool) + refresh headroom.  A selection runs only when fewer than a tile of
+// free slots remain, so each absorbs >= max(k', headroom) survivors.  With the
+// default headroom a capacity just above 512 or 1024 keys is trimmed to it
+// when that still leaves >= 128 keys of headroom: up to 1024 keys the
+// selection holds the whole pool in registers.
 int pool_capacity(int kp, int headroom = kTuneDefaultHeadroom) {
-  return (int)round_up(kp + kHalfN + std::max(kp, headroom), 32);
+  int P = (int)round_up(kp + kPoolRoom + std::max(kp, headroom), 32);
+  if (headroom == kTuneDefaultHeadroom) {
+    for (int lim : {512, 1024})
+      if (P > lim && kp + kPoolRoom + 128 <= lim && P <= lim + lim / 2) P = lim;
+  }
+  return P;
 }
 
 struct Timing {
@@ -302,7 +309,7 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
   FusedPlan plan;
   plan_fused(nq, (int)ix->n, ix->dres->num_sms, &plan, tp.split_q4);
   const long long nq_pad = round_up(nq, kBM);
-  const size_t pool_lists = (size_t)plan.num_qblocks * kBM * plan.units_per_block * 2;
+  const size_t pool_lists = (size_t)plan.num_qblocks * kBM * plan.units_per_block;
 
   Carve c(extra_base);
   __nv_bfloat16* qh = c.take<__nv_bfloat16>((size_t)nq_pad * ix->ld16);
@@ -409,7 +416,7 @@ size_t search_workspace_bytes(const curplsh_index* ix, int nq, int k, int form, 
   FusedPlan plan;
   plan_fused(nq, (int)ix->n, ix->dres->num_sms, &plan, tp.split_q4);
   const long long nq_pad = round_up(nq, kBM);
-  const size_t pool_lists = (size_t)plan.num_qblocks * kBM * plan.units_per_block * 2;
+  const size_t pool_lists = (size_t)plan.num_qblocks * kBM * plan.units_per_block;
   size_t b = 0;
   auto add = [&](size_t bytes) { b = (size_t)round_up((long long)b, 256) + bytes; };
   add((size_t)nq_pad * ix->ld16 * 2);

@@ -74,6 +74,7 @@ constexpr int kNumThreads = 320;  // warp 0 TMA producer, warp 1 MMA issuer, war
 // and the accumulator is ||q||^2 + ||x||^2 - 2 q.x directly.
 constexpr int kAugCols = 6;
 constexpr int kEpiWarps = 8;
+constexpr int kPoolRoom = kBN;  // free slots a candidate pool keeps for the next tile (both halves)
 
 // One work item of the fused pass: a query batch against one resident
 // database.  A launch serves a list of items that share the form and the

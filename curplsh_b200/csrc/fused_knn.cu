@@ -91,6 +91,7 @@ struct SmemLayout {
   int stages;
   uint32_t bar_off;    // offset of the barrier block
   uint32_t hist_off;   // warp-private radix histograms
+  uint32_t pool_off;   // per-row candidate pool counts and bounds
   uint32_t total;      // dynamic smem bytes requested (includes 1 KB alignment slack)
 };
 
@@ -106,7 +107,7 @@ __host__ __device__ inline SmemLayout make_layout(int form, int d) {
   // the tail runs the hi x hi product alone, which is exact only for those
   L.tail_narrow = folded && (d % 64 == 0);
   // everything below the barrier block must fit the 227 KB opt-in limit
-  const uint32_t budget = 227u * 1024u - 256u - (uint32_t)kEpiWarps * 256u * 4u - 1024u;
+  const uint32_t budget = 227u * 1024u - 256u - (uint32_t)kEpiWarps * 256u * 4u - 1024u - 1024u;
   const int nreg = L.nkc - (L.tail_narrow ? 1 : 0);
   const uint32_t a_res = (uint32_t)nreg * a_parts * kAChunkBytes + (L.tail_narrow ? kATailBytes : 0u);
   // a stage = one regular K chunk of the tile; the last one also carries the tail
@@ -125,7 +126,8 @@ __host__ __device__ inline SmemLayout make_layout(int form, int d) {
   L.stages = s < 2 ? 2 : (s > 8 ? 8 : s);
   L.bar_off = L.a_bytes + (uint32_t)L.stages * L.stage_bytes;
   L.hist_off = L.bar_off + 256;  // barriers: 2*8 + 6 mbarriers + tmem slot + flags < 256 B
-  L.total = L.hist_off + kEpiWarps * 256 * 4 + 1024;
+  L.pool_off = L.hist_off + kEpiWarps * 256 * 4;
+  L.total = L.pool_off + 1024 + 1024;
   return L;
 }
 
@@ -465,11 +467,21 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
     }
   } else {
     // ------------------------------------------------------------ epilogue
+    // Warps ew and ew + 4 read the same TMEM lanes (queries) and split each
+    // tile's columns into halves g = 0, 1.  They share ONE candidate pool per
+    // (query, unit): appends reserve slots with a shared-memory counter, and at
+    // every tile end the pair meets at a named barrier, splits the pools that
+    // need a selection between them, and meets again.  A shared pool sees
+    // both halves' rows, so its bound tightens as one pool over the whole
+    // tile would -- about half the survivors and selections of a pool per half.
     const int ew = warp - 2;       // 0..7
     const int g = ew >> 2;         // which 128-column half of each tile
     const int lg = warp & 3;       // TMEM lane group this warp may access
     const int row = lg * 32 + lane;
+    const int pair_bar = 1 + lg;   // named barrier of the two warps of lane group lg
     uint32_t* hist = hist_all + ew * 256;
+    int* cnt_s = reinterpret_cast<int*>(smem + L.pool_off);             // [128] pool counts
+    float* thr_s = reinterpret_cast<float*>(smem + L.pool_off) + kBM;   // [128] pool bounds
     const uint32_t lane_base = (uint32_t)(lg * 32) << 16;
     UnitWalk walk(blockIdx.x, B);
     int ii, qb, t0, t1, u_ord;
@@ -491,7 +503,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
       const FusedItem& p = A.items[ii];
       const int P = p.pool_cap;
       const int U = p.units_per_block;
-      if (u_ord < 0 || u_ord >= U) {
+      if (u_ord < 0 || u_ord >= U) {  // identical in every epilogue warp: both of a pair leave here
         raise_abort(abort_flag, B.status, kErrBadSchedule);
         break;
       }
@@ -502,62 +514,53 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
       if (Tr::kFP8) m2s = valid ? -2.f * p.q_scale[q] : 0.f;
       const size_t pool_row0 = (size_t)qb * kBM;  // pool index of lane-group row 0 is added per lane
       auto pool_of = [&](int r) -> uint64_t* {
-        return p.pools + (((pool_row0 + (size_t)r) * U + (size_t)u_ord) * 2 + (size_t)g) * (size_t)P;
+        return p.pools + ((pool_row0 + (size_t)r) * U + (size_t)u_ord) * (size_t)P;
       };
       uint64_t* pool = pool_of(row);
-      int n = 0;
+      // a new unit starts with an empty pool (the previous unit's last barrier
+      // ordered every use of the old state before this)
+      if (g == 0) {
+        cnt_s[row] = 0;
+        thr_s[row] = 3.402823466e38f;
+      }
+      bar_sync_named(pair_bar, 64);
       float thr = 3.402823466e38f;  // FLT_MAX: admits every finite distance until a pool fills
 
-      // Bounds shared between pools of this query: q_bound holds the smallest
-      // k'-th key distance any pool has reached; q_bound_half[2q+h] the
-      // smallest (k'/2)-th of any pool of half h.  Pools of different halves
-      // cover disjoint rows, so max(half 0, half 1) bounds the k'-th of their
-      // union -- about as tight as one pool over both halves.
-      uint32_t* qbh = p.q_bound_half + 2 * (size_t)(valid ? q : 0);
+      // Selections of the pools in `need` (lane bits of this lane group; warp g
+      // owns the pools of lanes with parity g, so the pair never touches the
+      // same pool's state).  Each keeps `keep` keys, records the pool's new
+      // count and bound in shared memory and publishes a full set's k'-th
+      // distance to q_bound.
       auto refresh = [&](uint32_t need, int keep) {
         STAT_BEGIN(tr);
-        STAT_INC(st_nref, __popc(need));
         while (need) {
           const int src = __ffs(need) - 1;
           need &= need - 1;
-          const int n_src = __shfl_sync(0xffffffffu, n, src);
+          STAT_INC(st_nref, 1);
+          const int r = lg * 32 + src;
+          const int n_src = cnt_s[r];
           int kept = 0;
           uint64_t half_key = 0;
-          const uint64_t kmax =
-              warp_select_keep_any(pool_of(lg * 32 + src), n_src < P ? n_src : P, keep, P, hist, kept, half_key);
+          const uint64_t kmax = warp_select_keep_any(pool_of(r), n_src < P ? n_src : P, keep, P, hist, kept, half_key);
           if (lane == src) {
-            n = kept;
             const uint32_t ord = (uint32_t)(kmax >> 32);
-            thr = fminf(thr, thr_from<Tr::kFolded>(ord2f(ord), qn));
+            cnt_s[r] = kept;
+            thr_s[r] = fminf(thr_s[r], thr_from<Tr::kFolded>(ord2f(ord), qn));
             // only a full set of k' keys bounds the global k'-th distance
-            if (kept >= p.kprime) {
-              atomicMin(&p.q_bound[q], ord);
-              atomicMin(&qbh[g], (uint32_t)(half_key >> 32));
-            }
+            if (kept >= p.kprime) atomicMin(&p.q_bound[q], ord);
           }
         }
         STAT_END(tr, st_refresh);
       };
 
-      // shared bounds are L2 round trips: load them one tile ahead
-      uint32_t nb_ob = kOrdInf, nb_h0 = kOrdInf, nb_h1 = kOrdInf;
-      if (valid) {
-        nb_ob = ld_relaxed_u32(&p.q_bound[q]);
-        nb_h0 = ld_relaxed_u32(&qbh[0]);
-        nb_h1 = ld_relaxed_u32(&qbh[1]);
-      }
+      // the shared bound is an L2 round trip: load it one tile ahead
+      uint32_t nb_ob = kOrdInf;
+      if (valid) nb_ob = ld_relaxed_u32(&p.q_bound[q]);
       for (int t = t0; t < t1; ++t, ++tc) {
         const uint32_t slot = tc & 1u, use = tc >> 1;
-        {
-          const uint32_t hb = nb_h0 > nb_h1 ? nb_h0 : nb_h1;  // both halves reported (else kOrdInf)
-          const uint32_t b = nb_ob < hb ? nb_ob : hb;
-          if (b != kOrdInf) thr = fminf(thr, thr_from<Tr::kFolded>(ord2f(b), qn));
-          if (valid) {
-            nb_ob = ld_relaxed_u32(&p.q_bound[q]);
-            nb_h0 = ld_relaxed_u32(&qbh[0]);
-            nb_h1 = ld_relaxed_u32(&qbh[1]);
-          }
-        }
+        thr = fminf(thr, thr_s[row]);
+        if (nb_ob != kOrdInf) thr = fminf(thr, thr_from<Tr::kFolded>(ord2f(nb_ob), qn));
+        if (valid) nb_ob = ld_relaxed_u32(&p.q_bound[q]);
         // FP8: this half tile's database norms and scales, loaded before the
         // accumulator wait (their latency overlaps it) and staged in the
         // warp's histogram area, which is free outside a refresh
@@ -571,12 +574,11 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
           }
         }
         STAT_BEGIN(tw);
-        if (!wait_or_abort(&acc_full[slot], use & 1u, abort_flag)) {
-          raise_abort(abort_flag, B.status, kErrWaitTimeout);
-          ok = false;
-          break;
-        }
+        bool got = wait_or_abort(&acc_full[slot], use & 1u, abort_flag);
+        if (!got) raise_abort(abort_flag, B.status, kErrWaitTimeout);
         STAT_END(tw, st_wait);
+        // an aborting warp skips the tile but still meets its partner below
+        if (got) {
         STAT_BEGIN(tfl);
         tc_fence_after();
         const int colh = t * kBN + g * kHalfN;
@@ -654,6 +656,12 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
             // A lane rarely has more than one survivor per 32 columns: take the
             // first of each half with a register select tree (no local memory),
             // a second one the same way, and stash only for the rare rest.
+            // slots for this lane's survivors of the 64 columns, reserved at once
+            int n = 0;
+            {
+              const int c = __popc(ma) + __popc(mb);
+              if (c) n = atomicAdd(&cnt_s[row], c);
+            }
             auto take = [&](uint32_t& m, const float (&dv)[32], int c0) {
               if (m) {
                 const int j = __ffs(m) - 1;
@@ -692,18 +700,31 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
         __syncwarp();
         if (lane == 0) mbar_arrive(&acc_empty[slot]);
         STAT_END(tfl, st_filter);
-        if (n > P) atomicOr(B.status, kErrPoolOverflow);
-        // a pool must have room for the next tile's half (kHalfN columns)
-        refresh(__ballot_sync(0xffffffffu, n > P - kHalfN), p.kprime);
+        }  // got
+        // meet the partner warp: leave together if either aborted
+        if (bar_red_or(pair_bar, 64, !got || *abort_flag != 0)) {
+          ok = false;
+          break;
+        }
+        // pools that may not have room for the next tile (both halves), or, at
+        // the unit's end, every pool above k' (the merge pass reads at most k'
+        // keys' worth beyond what it needs)
+        const int lim = t + 1 < t1 ? P - kBN : p.kprime;
+        const bool mine = (lane & 1) == g;
+        const int cn = mine ? cnt_s[row] : 0;
+        if (cn > P) atomicOr(B.status, kErrPoolOverflow);
+        refresh(__ballot_sync(0xffffffffu, mine && valid && cn > lim), p.kprime);
+        bar_sync_named(pair_bar, 64);
       }
       if (!ok) break;
-      refresh(__ballot_sync(0xffffffffu, n > p.kprime), p.kprime);
       // a refresh may keep a few more than k' keys (unsorted): record them all;
       // the merge pass selects exactly
-      if (valid) {
-        p.pool_counts[((pool_row0 + row) * U + u_ord) * 2 + g] = n < P ? n : P;
-        if (gap) p.pool_counts[((pool_row0 + row) * U + u_ord - 1) * 2 + g] = 0;
+      if (valid && g == 0) {
+        const int cn = cnt_s[row];
+        p.pool_counts[(pool_row0 + row) * U + u_ord] = cn < P ? cn : P;
+        if (gap) p.pool_counts[(pool_row0 + row) * U + u_ord - 1] = 0;
       }
+      bar_sync_named(pair_bar, 64);  // the counts are read before the next unit resets them
     }
     if (lane == 0) {
       STAT_FLUSH(kStatEpiWaitAccFull, st_wait);

@@ -117,9 +117,9 @@ __global__ void __launch_bounds__(kMergeThreads) merge_rerank_kernel(const __gri
   const long long W = m.work_per_cta;
   const long long first = (m.work_begin + (long long)qb * T) / W;
   const long long last = (m.work_begin + (long long)(qb + 1) * T - 1) / W;
-  // an empty database has no pools; otherwise one list per unit and half
-  const int nlists = T > 0 ? 2 * (int)(last - first + 1 + (T - 1) / m.split_tiles) : 0;
-  const size_t list0 = ((size_t)qb * kBM + row) * U * 2;  // pool-list index of (u=0, h=0)
+  // an empty database has no pools; otherwise one list per unit
+  const int nlists = T > 0 ? (int)(last - first + 1 + (T - 1) / m.split_tiles) : 0;
+  const size_t list0 = ((size_t)qb * kBM + row) * U;  // pool-list index of unit 0
   // Final bound of the fused pass on this query's k'-th coarse distance: the
   // smallest k'-th of any pool, and the larger of the per-half (k'/2)-th
   // bounds.  Every key of the k' smallest has a distance <= it.
@@ -303,17 +303,17 @@ cudaError_t launch_merge_batch(MergeItem* items, int n, int d, uint32_t* status,
   int kp2 = 32;  // >= 32 keeps the shared-memory carve 16-byte aligned
   while (kp2 < kpmax) kp2 <<= 1;
   a.kp2 = kp2;
-  // A pool can bound the k'-th distance only if a unit's half covers at least
-  // k' rows; without such pools there is nothing to prefilter with, and the
+  // A pool can bound the k'-th distance only if a unit covers at least k'
+  // rows; without such pools there is nothing to prefilter with, and the
   // launch keeps the smaller shared-memory footprint (higher occupancy).
   bool bounded = false;
   for (int i = 0; i < n; ++i) {
     long long len = std::min<long long>(items[i].split_tiles, items[i].work_per_cta);
     len = std::min<long long>(len, items[i].num_tiles);
-    bounded = bounded || (items[i].q_bound && len * kHalfN >= items[i].kprime);
+    bounded = bounded || (items[i].q_bound && len * kBN >= items[i].kprime);
   }
   a.pre_cap = bounded ? 2 * kp2 : 0;
-  a.lcnt_n = (2 * umax + 3) & ~3;
+  a.lcnt_n = (umax + 3) & ~3;
   bool vec4 = d % 4 == 0;
   for (int i = 0; i < n; ++i)
     vec4 = vec4 && (reinterpret_cast<uintptr_t>(items[i].queries) & 15) == 0 &&

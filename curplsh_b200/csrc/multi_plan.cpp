@@ -162,7 +162,7 @@ int MultiPlan::build(const curplsh_batch_item* items, int n, const std::vector<c
     x.o_bounds = o_bounds_ + bcur * sizeof(uint32_t);
     bcur += 3 * (size_t)x.nq_pad;
     if (v.n == 0) continue;
-    const size_t lists = (size_t)x.plan.num_qblocks * kBM * x.plan.units_per_block * 2;
+    const size_t lists = (size_t)x.plan.num_qblocks * kBM * x.plan.units_per_block;
     if (x.form != kFormFP8) x.o_qh = take((size_t)x.nq_pad * v.ld16 * 2);
     if (x.form == kFormExact) x.o_ql = take((size_t)x.nq_pad * v.ld16 * 2);
     if (x.form == kFormFP8) x.o_q8 = take((size_t)x.nq_pad * v.ld8);

@@ -136,7 +136,7 @@ int curplsh_index_search_profiled(curplsh_index* index, int64_t num, const float
  * serialised and the call returns when the results are written (it synchronises `stream`, NULL =
  * the legacy default stream).  The first call on a device looks up the array's device address, so
  * make it before any stream capture.  Requests whose working set exceeds the array are rejected
- * with CURPLSH_ERR_INVALID_ARG (roughly: num * (2*k'+128+max(k',256)) * 16 bytes must fit, k' the
+ * with CURPLSH_ERR_INVALID_ARG (roughly: num * (2*k'+256+max(k',256)) * 8 bytes must fit, k' the
  * candidate count); an index whose FP8 copy was never built by a regular FP8 search is rejected
  * with CURPLSH_ERR_STATE. */
 int curplsh_index_search_noalloc(curplsh_index* index, int64_t num, const float* queries, int k, int* indices,
