@@ -454,8 +454,11 @@ def run_serving(args, world, rank, local):
             gaps = rng.exponential(1.0 / mean_req, size=count)
             arrivals = np.cumsum(gaps) - gaps[0]
             lat, wall, _ = run_load(srv, sizes, list(arrivals))
+            slow = np.argsort(-lat)[:3]
             per_rate[str(rate)] = {"p50_ms": float(np.percentile(lat, 50) * 1e3),
                                    "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                                   "max_ms": float(lat.max() * 1e3),
+                                   "slowest": [[int(i), sizes[i], float(lat[i] * 1e3)] for i in slow],
                                    "achieved_queries_per_s": sum(sizes) / wall, "requests": count}
         st = srv.stats()
         srv.close()

@@ -259,13 +259,16 @@ int kprime_for(int form, int k, int rerank_factor, int64_t n) {
   return (int)kp;
 }
 
-// Pool capacity: k' kept keys + room for one tile (both halves append to the
-// pool) + refresh headroom.  A selection runs only when fewer than a tile of
+// Pool capacity: k' kept keys + room for one or two tiles (both halves append
+// to the pool; see pool_sync_tiles) + refresh headroom.  A selection runs only when fewer than a tile of
 // free slots remain, so each absorbs >= max(k', headroom) survivors.  With the
 // default headroom a capacity just above 512 or 1024 keys is trimmed to it
 // when that still leaves >= 128 keys of headroom: up to 1024 keys the
 // selection holds the whole pool in registers.
 int pool_capacity(int kp, int headroom = kTuneDefaultHeadroom) {
+  // room for two tiles between selections when the pool still fits registers
+  const int P2 = (int)round_up(kp + 2 * kPoolRoom + std::max(kp, headroom), 32);
+  if (P2 <= 1024) return P2;
   int P = (int)round_up(kp + kPoolRoom + std::max(kp, headroom), 32);
   if (headroom == kTuneDefaultHeadroom) {
     for (int lim : {512, 1024})
@@ -377,11 +380,11 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
             h[kStatEpiRefresh] / ctas / 8 / 1e6, h[kStatRefreshes], h[kStatSurvivors]);
     fprintf(stderr,
             "[fused-stats2] radix passes/refresh %.2f | slow chunks %llu (%.1f%% of warp-chunks) | loop iters/slow "
-            "chunk %.2f | tmem Mcycles/warp %.2f\n",
+            "chunk %.2f | tmem Mcycles/warp %.2f | pair barriers Mcycles/warp %.2f\n",
             h[kStatRefreshes] ? (double)h[kStatRadixPasses] / h[kStatRefreshes] : 0.0, h[kStatSlowChunks],
             100.0 * h[kStatSlowChunks] / (ctas * 8 * (double)plan.work_per_cta * 4),
             h[kStatSlowChunks] ? (double)h[kStatLoopIters] / h[kStatSlowChunks] : 0.0,
-            h[kStatTmemCycles] / ctas / 8 / 1e6);
+            h[kStatTmemCycles] / ctas / 8 / 1e6, h[kStatPairBarrier] / ctas / 8 / 1e6);
   }
 #endif
   tm->rec(3, st);

@@ -75,6 +75,9 @@ constexpr int kNumThreads = 320;  // warp 0 TMA producer, warp 1 MMA issuer, war
 constexpr int kAugCols = 6;
 constexpr int kEpiWarps = 8;
 constexpr int kPoolRoom = kBN;  // free slots a candidate pool keeps for the next tile (both halves)
+// Tiles between two selection points of a shared candidate pool: two when the
+// capacity leaves room for two tiles of appends above k' + 128, else one.
+__host__ __device__ inline int pool_sync_tiles(int cap, int kprime) { return cap >= kprime + 2 * kBN + 128 ? 2 : 1; }
 
 // One work item of the fused pass: a query batch against one resident
 // database.  A launch serves a list of items that share the form and the
@@ -130,6 +133,7 @@ enum FusedStat : int {
   kStatSlowChunks,             // warp-chunks (32 columns) that entered the survivor path
   kStatLoopIters,              // survivor-append loop iterations executed by warps
   kStatTmemCycles,             // epilogue warps (lane 0): cycles in TMEM loads + waits
+  kStatPairBarrier,            // epilogue warps (lane 0): cycles in the pair barriers
   kStatCount
 };
 

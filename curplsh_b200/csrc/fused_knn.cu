@@ -496,6 +496,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
     STAT_DECL(st_slow);
     STAT_DECL(st_iters);
     STAT_DECL(st_tmem);
+    STAT_DECL(st_bar);
 #ifdef CURPLSH_FUSED_STATS
     if (threadIdx.x == 64 && B.stats) g_radix_pass_counter = &B.stats[kStatRadixPasses];
 #endif
@@ -503,6 +504,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
       const FusedItem& p = A.items[ii];
       const int P = p.pool_cap;
       const int U = p.units_per_block;
+      const int S = pool_sync_tiles(P, p.kprime);
       if (u_ord < 0 || u_ord >= U) {  // identical in every epilogue warp: both of a pair leave here
         raise_abort(abort_flag, B.status, kErrBadSchedule);
         break;
@@ -618,10 +620,12 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
               const float4 sx = sx4[j4];
               float* dst = j4 < 8 ? da : db;
               const int o = (j4 & 7) * 4;
-              dst[o + 0] = fmaf(__uint_as_float(v[4 * j4 + 0]) * sx.x, m2s, xn.x);
-              dst[o + 1] = fmaf(__uint_as_float(v[4 * j4 + 1]) * sx.y, m2s, xn.y);
-              dst[o + 2] = fmaf(__uint_as_float(v[4 * j4 + 2]) * sx.z, m2s, xn.z);
-              dst[o + 3] = fmaf(__uint_as_float(v[4 * j4 + 3]) * sx.w, m2s, xn.w);
+              // fmaf(acc * s_x, -2 s_q, ||x||^2) on column pairs
+              float p0, p1, p2, p3;
+              mul2_f32(p0, p1, __uint_as_float(v[4 * j4 + 0]), __uint_as_float(v[4 * j4 + 1]), sx.x, sx.y);
+              mul2_f32(p2, p3, __uint_as_float(v[4 * j4 + 2]), __uint_as_float(v[4 * j4 + 3]), sx.z, sx.w);
+              fma2_f32(dst[o + 0], dst[o + 1], p0, p1, m2s, m2s, xn.x, xn.y);
+              fma2_f32(dst[o + 2], dst[o + 3], p2, p3, m2s, m2s, xn.z, xn.w);
             }
           }
           // survivor masks, each OR-combined in four independent partial masks
@@ -701,20 +705,27 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
         if (lane == 0) mbar_arrive(&acc_empty[slot]);
         STAT_END(tfl, st_filter);
         }  // got
-        // meet the partner warp: leave together if either aborted
-        if (bar_red_or(pair_bar, 64, !got || *abort_flag != 0)) {
+        // every S tiles (and at the unit's end) meet the partner warp; leave
+        // together if either aborted
+        if ((t - t0 + 1) % S != 0 && t + 1 < t1) continue;
+        STAT_BEGIN(tb1);
+        const bool leave = bar_red_or(pair_bar, 64, !got || *abort_flag != 0);
+        STAT_END(tb1, st_bar);
+        if (leave) {
           ok = false;
           break;
         }
-        // pools that may not have room for the next tile (both halves), or, at
-        // the unit's end, every pool above k' (the merge pass reads at most k'
-        // keys' worth beyond what it needs)
-        const int lim = t + 1 < t1 ? P - kBN : p.kprime;
+        // pools that may not have room for the next S tiles (both halves),
+        // or, at the unit's end, every pool above k' (the merge pass reads at
+        // most k' keys' worth beyond what it needs)
+        const int lim = t + 1 < t1 ? P - S * kBN : p.kprime;
         const bool mine = (lane & 1) == g;
         const int cn = mine ? cnt_s[row] : 0;
         if (cn > P) atomicOr(B.status, kErrPoolOverflow);
         refresh(__ballot_sync(0xffffffffu, mine && valid && cn > lim), p.kprime);
+        STAT_BEGIN(tb2);
         bar_sync_named(pair_bar, 64);
+        STAT_END(tb2, st_bar);
       }
       if (!ok) break;
       // a refresh may keep a few more than k' keys (unsorted): record them all;
@@ -734,6 +745,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
       STAT_FLUSH(kStatSlowChunks, st_slow);
       STAT_FLUSH(kStatLoopIters, st_iters);
       STAT_FLUSH(kStatTmemCycles, st_tmem);
+      STAT_FLUSH(kStatPairBarrier, st_bar);
     }
     STAT_FLUSH(kStatSurvivors, st_surv);
   }

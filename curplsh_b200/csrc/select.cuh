@@ -259,7 +259,7 @@ __device__ __forceinline__ uint64_t warp_select_keep_sampled(uint64_t* pool, int
   }
   uint32_t c_keep = 0, c_half = 0;
   const uint64_t bound = warp_sample_find<E>(key, smp, n, (uint32_t)keep, c_keep);
-  if (c_keep < (uint32_t)keep || bound == kKeyEmpty || (int)c_keep > cap - kPoolRoom) {
+  if (c_keep < (uint32_t)keep || bound == kKeyEmpty || (int)c_keep > cap - pool_sync_tiles(cap, keep) * kBN) {
     // samples too coarse to free a tile of room: exact selection
     __syncwarp();
     uint64_t hb;
@@ -413,7 +413,7 @@ __device__ __noinline__ uint64_t warp_refresh_pool(uint64_t* pool, int n, int ke
   uint32_t c_keep = 0;
   uint64_t bound = warp_stream_sample_find(pool, n, smp, (uint32_t)keep, c_keep);
   uint64_t kmax;
-  if (c_keep < (uint32_t)keep || (int)c_keep > cap - kPoolRoom) {
+  if (c_keep < (uint32_t)keep || (int)c_keep > cap - pool_sync_tiles(cap, keep) * kBN) {
     // samples too coarse to free a tile of room: exact radix selection
     bound = warp_stream_bound(pool, n, kKeyEmpty - 1, (uint32_t)keep, hist);
     kmax = warp_stream_max_le(pool, n, bound);
