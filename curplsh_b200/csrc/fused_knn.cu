@@ -157,7 +157,8 @@ struct FusedArgs {
 };
 
 // Walks the contiguous range [cta*W, min(total,(cta+1)*W)) of the flattened
-// (item, query block, tile) space as units (item, query block, [t0, t1)).  A
+// (item, query block, tile position) space as units (item, query block,
+// [t0, t1)); positions map to database tiles through a per-block rotation.  A
 // unit also ends at every multiple of the item's split length L, so no unit
 // gathers candidates from more than L tiles (a split-N knob: longer units
 // mean fewer pool lists for the merge but more in-pool selections).
@@ -172,7 +173,8 @@ struct UnitWalk {
     end = pos + W < B.total_work ? pos + W : B.total_work;
   }
   template <int MAXI>
-  __device__ bool next(const FusedArgs<MAXI>& A, int& item, int& qb, int& t0, int& t1, int& u_ord, bool& gap) {
+  __device__ bool next(const FusedArgs<MAXI>& A, int& item, int& qb, int& t0, int& t1, int& u_ord, bool& gap,
+                       int& rot) {
     if (pos >= end) return false;
     while (ii < A.B.num_items && A.items[ii].work_end <= pos) ++ii;
     if (ii >= A.B.num_items) return false;
@@ -189,6 +191,15 @@ struct UnitWalk {
     const long long base = wb + (long long)qb * T;
     u_ord = (int)(pos / W - base / W) + t0 / Ls;
     gap = t0 > 0 && t0 % Ls == 0 && pos % W == 0;
+    // Position j of the block is database tile (j - rot) mod T, where rot is
+    // where the first CTA range starting inside this block begins: every such
+    // CTA then reads tiles 0, 1, 2, ... from the start, in step with the
+    // others, so concurrent CTAs share the database tiles in L2 (a contiguous
+    // assignment alone would have them at spread-out offsets).
+    {
+      const long long first = (base + W - 1) / W * W - base;
+      rot = first < T ? (int)first : 0;
+    }
     item = ii;
     pos += len;
     return true;
@@ -321,12 +332,12 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
       const uint64_t pol_db = l2_policy_evict_first();
       const uint64_t pol_q = l2_policy_evict_last();
       UnitWalk walk(blockIdx.x, B);
-      int ii, qb, t0, t1, u_ord, unit = 0;
+      int ii, qb, t0, t1, u_ord, rot, unit = 0;
       bool gap;
       uint32_t it = 0;
       bool ok = true;
       STAT_DECL(st_wait);
-      while (ok && walk.next(A, ii, qb, t0, t1, u_ord, gap)) {
+      while (ok && walk.next(A, ii, qb, t0, t1, u_ord, gap, rot)) {
         const CUtensorMap* mp = maps_of(ii);
         const CUtensorMap& tm_q_hi = mp[kMapQHi];
         const CUtensorMap& tm_q_lo = mp[kMapQLo];
@@ -352,6 +363,8 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
         }
         const int nreg = L.nkc - (L.tail_narrow ? 1 : 0);
         for (int t = t0; t < t1 && ok; ++t) {
+          const int T_i = A.items[ii].num_tiles;
+          const int tx_row = ((t - rot + T_i) % T_i) * kBN;  // database tile of position t
           for (int kc = 0; kc < nreg; ++kc, ++it) {
             const int s = (int)(it % (uint32_t)S);
             STAT_BEGIN(tw);
@@ -367,14 +380,14 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
             if (with_tail) tx += kBTailBytes + (L.a_stream ? kATailBytes : 0u);
             mbar_arrive_expect_tx(&full[s], tx);
             for (int part = 0; part < Tr::kBParts; ++part)
-              tma_load_2d(st + part * kBChunkBytes, part ? &tm_x_lo : &tm_x_hi, &full[s], kc * KC, t * kBN, pol_db);
+              tma_load_2d(st + part * kBChunkBytes, part ? &tm_x_lo : &tm_x_hi, &full[s], kc * KC, tx_row, pol_db);
             if (L.a_stream)
               for (int part = 0; part < Tr::kAParts; ++part)
                 tma_load_2d(st + stage_a_off<Tr::kAParts, Tr::kBParts>(part), part ? &tm_q_lo : &tm_q_hi, &full[s],
                             kc * KC, qb * kBM, pol_q);
             if (with_tail) {
               uint8_t* tl = st + stage_tail_off<Tr::kAParts, Tr::kBParts>(L);
-              tma_load_2d(tl, &tm_x_tail, &full[s], nreg * KC, t * kBN, pol_db);
+              tma_load_2d(tl, &tm_x_tail, &full[s], nreg * KC, tx_row, pol_db);
               if (L.a_stream) tma_load_2d(tl + kBTailBytes, &tm_q_tail, &full[s], nreg * KC, qb * kBM, pol_q);
             }
           }
@@ -389,13 +402,13 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
       constexpr uint32_t fmt = Tr::kFP8 ? 0u : 1u;  // e4m3 : bf16
       constexpr uint32_t idesc = make_idesc(fmt, fmt, kBM, kBN);
       UnitWalk walk(blockIdx.x, B);
-      int ii, qb, t0, t1, u_ord, unit = 0;
+      int ii, qb, t0, t1, u_ord, rot, unit = 0;
       bool gap;
       uint32_t it = 0, tc = 0;
       bool ok = true;
       STAT_DECL(st_full);
       STAT_DECL(st_acc);
-      while (ok && walk.next(A, ii, qb, t0, t1, u_ord, gap)) {
+      while (ok && walk.next(A, ii, qb, t0, t1, u_ord, gap, rot)) {
         if (!L.a_stream) {
           if (!wait_or_abort(a_full, unit & 1, abort_flag)) {
             raise_abort(abort_flag, B.status, kErrWaitTimeout);
@@ -484,7 +497,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
     float* thr_s = reinterpret_cast<float*>(smem + L.pool_off) + kBM;   // [128] pool bounds
     const uint32_t lane_base = (uint32_t)(lg * 32) << 16;
     UnitWalk walk(blockIdx.x, B);
-    int ii, qb, t0, t1, u_ord;
+    int ii, qb, t0, t1, u_ord, rot;
     bool gap;
     uint32_t tc = 0;
     bool ok = true;
@@ -500,7 +513,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
 #ifdef CURPLSH_FUSED_STATS
     if (threadIdx.x == 64 && B.stats) g_radix_pass_counter = &B.stats[kStatRadixPasses];
 #endif
-    while (ok && walk.next(A, ii, qb, t0, t1, u_ord, gap)) {
+    while (ok && walk.next(A, ii, qb, t0, t1, u_ord, gap, rot)) {
       const FusedItem& p = A.items[ii];
       const int P = p.pool_cap;
       const int U = p.units_per_block;
@@ -560,6 +573,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
       if (valid) nb_ob = ld_relaxed_u32(&p.q_bound[q]);
       for (int t = t0; t < t1; ++t, ++tc) {
         const uint32_t slot = tc & 1u, use = tc >> 1;
+        const int tphys = (t - rot + p.num_tiles) % p.num_tiles;  // database tile of position t
         thr = fminf(thr, thr_s[row]);
         if (nb_ob != kOrdInf) thr = fminf(thr, thr_from<Tr::kFolded>(ord2f(nb_ob), qn));
         if (valid) nb_ob = ld_relaxed_u32(&p.q_bound[q]);
@@ -570,7 +584,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
         if (Tr::kFP8) {
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
-            const int c = t * kBN + g * kHalfN + lane + 32 * i;  // < nb_pad: rows are padded to whole tiles
+            const int c = tphys * kBN + g * kHalfN + lane + 32 * i;  // < nb_pad: rows are padded to whole tiles
             pxn[i] = __ldg(p.db_norms + c);
             psx[i] = __ldg(p.db_scale + c);
           }
@@ -583,7 +597,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
         if (got) {
         STAT_BEGIN(tfl);
         tc_fence_after();
-        const int colh = t * kBN + g * kHalfN;
+        const int colh = tphys * kBN + g * kHalfN;
         float* colv = reinterpret_cast<float*>(hist);  // [128] norms, then [128] scales
         if (Tr::kFP8) {
           __syncwarp();
