@@ -261,7 +261,9 @@ def run_batched(args, world, rank, local):
         recs = autotune.tune_batch(items, precision=precision, reps=2, stream=stream)
         tuned = {"buckets": len(recs), "tuning_s": time.perf_counter() - t0,
                  "untuned_ms_per_step": e0.elapsed_time(e1) / args.steps,
-                 "changed": sum(1 for r in recs if (r["split_q4"], r["pool_headroom"]) != autotune.DEFAULT)}
+                 "changed": sum(1 for r in recs if (r["split_q4"], r["pool_headroom"]) != autotune.DEFAULT),
+                 "picks": {r["bucket"]: [r["split_q4"], r["pool_headroom"], round(r["ms"], 3), round(r["default_ms"], 3)]
+                           for r in recs}}
     batch = cb.SearchBatch(items, precision=precision)
     kernels, ws_bytes = batch.info()
     # correctness: every item equals its search alone; a query sample against the oracle

@@ -216,7 +216,8 @@ struct curplsh_index {
   __nv_bfloat16* xl = nullptr;    // [n_pad x ld16]
   uint8_t* x8 = nullptr;          // [n_pad x ld8]   (built on first FP8 search)
   float* xs = nullptr;            // [n_pad]
-  uint32_t* status = nullptr;     // device error word
+  uint32_t* status = nullptr;     // device words: [0] error status, [1] nonzero if a row is not exactly BF16
+  bool bf16_exact = false;        // every stored value is exactly a BF16 value (rerank reads xh)
   long long generation = 0;       // bumped whenever the prepared database changes (add, reset)
   cudaEvent_t order_ev = nullptr; // orders default-stream searches after the legacy stream
   std::map<cudaStream_t, std::unique_ptr<StreamWorkspace>> ws;
@@ -310,7 +311,7 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
   const TuneParams tp = tune_lookup(form, d, k, nq);
   const int P = pool_capacity(kp, tp.headroom);
   FusedPlan plan;
-  plan_fused(nq, (int)ix->n, ix->dres->num_sms, &plan, tp.split_q4);
+  plan_fused(nq, (int)ix->n, ix->dres->num_sms, &plan, default_split_q4(tp, P));
   const long long nq_pad = round_up(nq, kBM);
   const size_t pool_lists = (size_t)plan.num_qblocks * kBM * plan.units_per_block;
 
@@ -403,6 +404,10 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
   m.queries = q_dev;
   m.db = ix->x32;
   m.ld_db = d;
+  if (ix->bf16_exact) {
+    m.db16 = ix->xh;
+    m.ld16 = ix->ld16;
+  }
   m.out_idx = out_idx;
   m.out_dist = out_dist;
   m.status = ix->status;
@@ -417,7 +422,7 @@ size_t search_workspace_bytes(const curplsh_index* ix, int nq, int k, int form, 
   const TuneParams tp = tune_lookup(form, ix->dim, k, nq);
   const int P = pool_capacity(kp, tp.headroom);
   FusedPlan plan;
-  plan_fused(nq, (int)ix->n, ix->dres->num_sms, &plan, tp.split_q4);
+  plan_fused(nq, (int)ix->n, ix->dres->num_sms, &plan, default_split_q4(tp, P));
   const long long nq_pad = round_up(nq, kBM);
   const size_t pool_lists = (size_t)plan.num_qblocks * kBM * plan.units_per_block;
   size_t b = 0;
@@ -550,6 +555,7 @@ int index_lock_view(curplsh_index* ix, IndexView* v) {
   v->x8 = ix->x8;
   v->xs = ix->xs;
   v->generation = ix->generation;
+  v->bf16_exact = ix->bf16_exact;
   v->stream = ix->dres->def;
   return CURPLSH_OK;
 }
@@ -704,8 +710,8 @@ int curplsh_index_bf_create(curplsh_resources* r, int dim, const curplsh_bf_conf
   ix->ld8 = round_up(dim, 16);
   r->refs.fetch_add(1);
   DeviceScope scope(c.device);
-  cudaError_t e = cudaMalloc(&ix->status, sizeof(uint32_t));
-  if (e == cudaSuccess) e = cudaMemset(ix->status, 0, sizeof(uint32_t));
+  cudaError_t e = cudaMalloc(&ix->status, 2 * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemset(ix->status, 0, 2 * sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ix->order_ev, cudaEventDisableTiming);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -789,7 +795,9 @@ int curplsh_index_add(curplsh_index* ix, int64_t num, const float* data) {
   const float inf = __builtin_huge_valf();
   CUDA_TRY(launch_prep_rows(x32 + (size_t)n_old * d, d, (int)num, pad_new - n_old, d, xn + n_old, inf,
                             xh + (size_t)n_old * ix->ld16, xl + (size_t)n_old * ix->ld16, ix->ld16, nullptr,
-                            nullptr, ix->ld8, st, kAugDatabase));
+                            nullptr, ix->ld8, st, kAugDatabase, ix->status + 1));
+  uint32_t lo_flag = 1;
+  CUDA_TRY(cudaMemcpyAsync(&lo_flag, ix->status + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaStreamSynchronize(st));
   // swap in
   float* old_x32 = ix->x32;
@@ -805,6 +813,7 @@ int curplsh_index_add(curplsh_index* ix, int64_t num, const float* data) {
   ix->xl = xl;
   ix->n = n_new;
   ix->n_pad = pad_new;
+  ix->bf16_exact = lo_flag == 0;  // the flag accumulates over every add since creation or reset
   ++ix->generation;
   return CURPLSH_OK;
 }
@@ -833,6 +842,8 @@ int curplsh_index_reset(curplsh_index* ix) {
   cudaStreamSynchronize(ix->dres->def);
   for (auto& kv : ix->ws) cudaStreamSynchronize(kv.first);
   ix->free_db();
+  ix->bf16_exact = false;
+  CUDA_TRY(cudaMemset(ix->status + 1, 0, sizeof(uint32_t)));
   ++ix->generation;
   return CURPLSH_OK;
 }

@@ -22,9 +22,16 @@ constexpr int kTuneMinHeadroom = 128;
 constexpr int kTuneMaxHeadroom = 8192;
 struct TuneParams {
   int split_q4 = 4;                      // unit length limit in quarters of the search's own CTA range W
-  int headroom = kTuneDefaultHeadroom;   // pool capacity = k' + 128 + max(k', headroom), rounded to 32
+  int headroom = kTuneDefaultHeadroom;   // pool capacity = k' + room + max(k', headroom), rounded to 32
+  bool tuned = false;                    // set by the autotuner (else the defaults below apply)
 };
 TuneParams tune_lookup(int form, int d, int k, long long nq);
+// Split used when a bucket was never tuned: pools above 1024 keys take the
+// streaming selection (several passes over global memory), so their units are
+// halved, leaving more of the selection to the merge pass.
+inline int default_split_q4(const TuneParams& t, int pool_cap) {
+  return t.tuned ? t.split_q4 : (pool_cap > 1024 ? 2 : 4);
+}
 // Unit length limit for an item whose own CTA range is w_own tiles (>= 1).
 inline int split_tiles_for(long long w_own, int split_q4) {
   const long long s = (w_own * split_q4 + 3) / 4;
@@ -115,9 +122,12 @@ cudaError_t launch_fused_batch(int form, const FusedItemSpec* specs, const Fused
 // database rows get [n1 n2 n3 1 1 1] after column d, query rows are stored as -2q
 // followed by [1 1 1 m1 m2 m3]; lo rows get zeros there.
 enum AugMode : int { kAugNone = 0, kAugDatabase = 1, kAugQuery = 2 };
+// `lo_nonzero` (optional) gets a nonzero value when some real row element is
+// not exactly representable in BF16 (its lo part is nonzero).
 cudaError_t launch_prep_rows(const float* x, long long ldx, int nrows, long long nrows_pad, int d, float* norms,
                              float pad_norm, __nv_bfloat16* hi, __nv_bfloat16* lo, long long ld16, uint8_t* f8,
-                             float* scale, long long ld8, cudaStream_t st, int aug = kAugNone);
+                             float* scale, long long ld8, cudaStream_t st, int aug = kAugNone,
+                             uint32_t* lo_nonzero = nullptr);
 
 // The same preparation for several row ranges of one dimension in a single
 // launch.  Every pointer points at the segment's first row; source rows have
@@ -150,6 +160,8 @@ struct MergeLaunch {
   const float* queries;   // [nq x d] fp32, row stride d
   const float* db;        // [nb x d] fp32, row stride ld_db
   long long ld_db;
+  const __nv_bfloat16* db16 = nullptr;  // see MergeItem
+  long long ld16 = 0;
   int* out_idx;
   float* out_dist;
   uint32_t* status;
@@ -175,6 +187,8 @@ struct MergeItem {
   const float* queries;    // [nq x d] fp32, row stride d
   const float* db;         // database rows fp32, row stride ld_db
   long long ld_db;
+  const __nv_bfloat16* db16;  // non-null: every row is exactly BF16; rerank reads these rows (stride ld16)
+  long long ld16;
   int* out_idx;            // [nq x k]
   float* out_dist;
 };
@@ -201,6 +215,7 @@ struct IndexView {
   const uint8_t* x8;
   const float* xs;
   long long generation;  // changes whenever add()/reset() replace the prepared database
+  bool bf16_exact;       // every stored value is exactly a BF16 value (xl is all zero)
   cudaStream_t stream;   // the index's default stream
 };
 // Locks the index (same lock as search/add) and fills `out`; unlock with index_unlock.

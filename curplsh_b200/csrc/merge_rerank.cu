@@ -17,6 +17,8 @@
 #include <algorithm>
 #include <cstring>
 
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 #include "fused_knn.h"
 
@@ -201,7 +203,41 @@ __global__ void __launch_bounds__(kMergeThreads) merge_rerank_kernel(const __gri
     const float* x0 = m.db + (size_t)i0 * m.ld_db;
     const float* x1 = m.db + (size_t)i1 * m.ld_db;
     float s0 = 0.f, s1 = 0.f;
-    if (a.vec4) {
+    if (m.db16) {
+      // rows exactly representable in BF16: read half the bytes; the same
+      // lane-to-element assignment and order as the FP32 path below
+      const __nv_bfloat16* b0 = m.db16 + (size_t)i0 * m.ld16;
+      const __nv_bfloat16* b1 = m.db16 + (size_t)i1 * m.ld16;
+      if (a.vec4) {
+        const float4* q4 = reinterpret_cast<const float4*>(qv);
+        const uint2* y0 = reinterpret_cast<const uint2*>(b0);
+        const uint2* y1 = reinterpret_cast<const uint2*>(b1);
+        for (int i = lane; i < d / 4; i += 32) {
+          const float4 qq = q4[i];
+          const uint2 u = __ldg(y0 + i), v = __ldg(y1 + i);
+          const float2 u01 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.x));
+          const float2 u23 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.y));
+          const float2 v01 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&v.x));
+          const float2 v23 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&v.y));
+          float t;
+          t = qq.x - u01.x; s0 = fmaf(t, t, s0);
+          t = qq.y - u01.y; s0 = fmaf(t, t, s0);
+          t = qq.z - u23.x; s0 = fmaf(t, t, s0);
+          t = qq.w - u23.y; s0 = fmaf(t, t, s0);
+          t = qq.x - v01.x; s1 = fmaf(t, t, s1);
+          t = qq.y - v01.y; s1 = fmaf(t, t, s1);
+          t = qq.z - v23.x; s1 = fmaf(t, t, s1);
+          t = qq.w - v23.y; s1 = fmaf(t, t, s1);
+        }
+      } else {
+        for (int i = lane; i < d; i += 32) {
+          const float qq = qv[i];
+          const float t0 = qq - __bfloat162float(b0[i]), t1 = qq - __bfloat162float(b1[i]);
+          s0 = fmaf(t0, t0, s0);
+          s1 = fmaf(t1, t1, s1);
+        }
+      }
+    } else if (a.vec4) {
       const float4* q4 = reinterpret_cast<const float4*>(qv);
       const float4* y0 = reinterpret_cast<const float4*>(x0);
       const float4* y1 = reinterpret_cast<const float4*>(x1);
@@ -347,6 +383,8 @@ cudaError_t launch_merge_rerank(const MergeLaunch& m, cudaStream_t st) {
   it.queries = m.queries;
   it.db = m.db;
   it.ld_db = m.ld_db;
+  it.db16 = m.db16;
+  it.ld16 = m.ld16;
   it.out_idx = m.out_idx;
   it.out_dist = m.out_dist;
   return launch_merge_batch(&it, 1, m.d, m.status, st);

@@ -134,7 +134,7 @@ int MultiPlan::build(const curplsh_batch_item* items, int n, const std::vector<c
         // as alone), so its in-pool selection work stays what it is alone
         const long long own = (long long)((x.nq + kBM - 1) / kBM) * ((specs[j].nb + kBN - 1) / kBN);
         specs[j].split_tiles = split_tiles_for(std::max<long long>(1, (own + num_sms - 1) / num_sms),
-                                               std::min(x.tune.split_q4, 4));
+                                               std::min(default_split_q4(x.tune, x.P), 4));
       }
       plan_fused_batch(specs.data(), (int)specs.size(), num_sms, plans.data(), &FL.bp);
       for (size_t j = 0; j < FL.fitems.size(); ++j) {
@@ -306,6 +306,8 @@ int MultiPlan::enqueue(cudaStream_t main, const std::vector<cudaStream_t>* branc
         m.queries = it.queries;
         m.db = v.x32;
         m.ld_db = v.dim;
+        m.db16 = v.bf16_exact ? v.xh : nullptr;
+        m.ld16 = v.ld16;
         m.out_idx = it.indices;
         m.out_dist = it.distances;
         by_class[cls].push_back(m);

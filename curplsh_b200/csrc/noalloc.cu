@@ -227,6 +227,10 @@ int search_noalloc_locked(const IndexView& v, int nq, const float* q, int k, int
   m.ld_db = v.dim;
   m.out_idx = out_idx;
   m.out_dist = out_dist;
+  if (v.bf16_exact) {
+    m.db16 = v.xh;
+    m.ld16 = v.ld16;
+  }
   m.status = status;
   NA_TRY(launch_merge_rerank(m, st));
   uint32_t host_status = 0;

@@ -55,7 +55,8 @@ __device__ __forceinline__ float aug_value(int aug, int c, float s) {
 __device__ __forceinline__ void prep_row(const float* __restrict__ x, long long ldx, long long r, int nrows, int d,
                                          float* __restrict__ norms, float pad_norm, __nv_bfloat16* __restrict__ hi,
                                          __nv_bfloat16* __restrict__ lo, long long ld16, uint8_t* __restrict__ f8,
-                                         float* __restrict__ scale, long long ld8, int vec4, int aug) {
+                                         float* __restrict__ scale, long long ld8, int vec4, int aug,
+                                         uint32_t* __restrict__ lo_nonzero = nullptr) {
   const int lane = threadIdx.x & 31;
   if (r >= nrows) {
     if (norms && lane == 0) norms[r] = pad_norm;
@@ -92,6 +93,7 @@ __device__ __forceinline__ void prep_row(const float* __restrict__ x, long long 
   if (!hi && !lo && !f8) return;
   // query rows of the augmented forms are stored as -2q (exact in BF16)
   const float hsc = aug == kAugQuery ? -2.f : 1.f;
+  bool lo_any = false;  // some element is not exactly a BF16 value
   float inv = 1.f;
   if (f8) {
     m = warp_max(m);
@@ -125,6 +127,7 @@ __device__ __forceinline__ void prep_row(const float* __restrict__ x, long long 
           pl.x = *reinterpret_cast<uint32_t*>(&c);
           pl.y = *reinterpret_cast<uint32_t*>(&e);
           *reinterpret_cast<uint2*>(lo + r * ld16 + 4 * i) = pl;
+          lo_any |= ((pl.x | pl.y) & 0x7FFF7FFFu) != 0u;  // ignore -0
         }
       }
       if (f8) {
@@ -148,7 +151,10 @@ __device__ __forceinline__ void prep_row(const float* __restrict__ x, long long 
           const float v = row[i];
           const __nv_bfloat16 h = __float2bfloat16_rn(v);
           hi[r * ld16 + i] = __float2bfloat16_rn(hsc * __bfloat162float(h));
-          if (lo) lo[r * ld16 + i] = __float2bfloat16_rn(hsc * (v - __bfloat162float(h)));
+          if (lo) {
+            lo[r * ld16 + i] = __float2bfloat16_rn(hsc * (v - __bfloat162float(h)));
+            lo_any |= v != __bfloat162float(h);
+          }
         } else {
           const int c = (int)(i - d);
           hi[r * ld16 + i] = __float2bfloat16_rn(aug && c < kAugCols ? aug_value(aug, c, s) : 0.f);
@@ -161,15 +167,17 @@ __device__ __forceinline__ void prep_row(const float* __restrict__ x, long long 
         f8[r * ld8 + i] = to_e4m3(v * inv);
       }
   }
+  if (lo_nonzero && __any_sync(0xffffffffu, lo_any) && lane == 0) atomicOr(lo_nonzero, 1u);
 }
 
 __global__ void __launch_bounds__(kPrepWarps * 32) prep_rows_kernel(
     const float* __restrict__ x, long long ldx, int nrows, long long nrows_pad, int d, float* __restrict__ norms,
     float pad_norm, __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, long long ld16,
-    uint8_t* __restrict__ f8, float* __restrict__ scale, long long ld8, int vec4, int aug) {
+    uint8_t* __restrict__ f8, float* __restrict__ scale, long long ld8, int vec4, int aug,
+    uint32_t* __restrict__ lo_nonzero) {
   const long long r = (long long)blockIdx.x * kPrepWarps + (threadIdx.x >> 5);
   if (r >= nrows_pad) return;
-  prep_row(x, ldx, r, nrows, d, norms, pad_norm, hi, lo, ld16, f8, scale, ld8, vec4, aug);
+  prep_row(x, ldx, r, nrows, d, norms, pad_norm, hi, lo, ld16, f8, scale, ld8, vec4, aug, lo_nonzero);
 }
 
 struct PrepSegmentArgs {
@@ -236,12 +244,12 @@ __global__ void fill_results_kernel(int* idx, float* dist, long long n) {
 
 cudaError_t launch_prep_rows(const float* x, long long ldx, int nrows, long long nrows_pad, int d, float* norms,
                              float pad_norm, __nv_bfloat16* hi, __nv_bfloat16* lo, long long ld16, uint8_t* f8,
-                             float* scale, long long ld8, cudaStream_t st, int aug) {
+                             float* scale, long long ld8, cudaStream_t st, int aug, uint32_t* lo_nonzero) {
   if (nrows_pad <= 0) return cudaSuccess;
   const int vec4 = (d % 4 == 0) && (ldx % 4 == 0) && ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
   const long long blocks = (nrows_pad + kPrepWarps - 1) / kPrepWarps;
   prep_rows_kernel<<<(unsigned)blocks, kPrepWarps * 32, 0, st>>>(x, ldx, nrows, nrows_pad, d, norms, pad_norm, hi,
-                                                                 lo, ld16, f8, scale, ld8, vec4, aug);
+                                                                 lo, ld16, f8, scale, ld8, vec4, aug, lo_nonzero);
   return cudaGetLastError();
 }
 

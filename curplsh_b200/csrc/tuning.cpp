@@ -67,7 +67,7 @@ int curplsh_tuning_set(int precision, int dim, int k, int64_t num_queries, int s
     return record_error(CURPLSH_ERR_INVALID_ARG,
                         "curplsh_tuning_set: split_q4 must be in [1, 64], pool_headroom in [128, 8192]");
   std::lock_guard<std::mutex> lk(g_mu);
-  g_table[key_of(precision, dim, k, num_queries)] = TuneParams{split_q4, pool_headroom};
+  g_table[key_of(precision, dim, k, num_queries)] = TuneParams{split_q4, pool_headroom, true};
   return CURPLSH_OK;
 }
 

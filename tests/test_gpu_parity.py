@@ -220,3 +220,27 @@ def test_deterministic_repeat(cb, res):
         b = ix.search_array(queries, 64)
         np.testing.assert_array_equal(a[1], b[1])
         np.testing.assert_array_equal(a[0], b[0])
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_bf16_exact_rows_rerank_identically(cb, res, form):
+    """An index whose values are all exactly BF16 reranks from its BF16 copy;
+    the same rows in an index that also holds one non-BF16 row (far away, so
+    never a neighbour) rerank from FP32.  Both must give identical results."""
+    import torch
+    rng = np.random.default_rng(31 + form)
+    n, nq, d, k = 5000, 64, 96, 20
+    base = torch.tensor(rng.standard_normal((n, d), dtype=np.float32)).bfloat16().float().numpy()
+    q = rng.standard_normal((nq, d), dtype=np.float32)
+    far = np.full((1, d), 1000.0, np.float32)
+    far[0, 0] = 1000.1  # not a BF16 value
+    a = make_index(cb, res, base, precision=form)
+    b = make_index(cb, res, np.concatenate([base, far]), precision=form)
+    da, ia = a.search_array(q, k)
+    db, ib = b.search_array(q, k)
+    np.testing.assert_array_equal(ia, ib)
+    np.testing.assert_array_equal(da, db)
+    rd, ri = oracle.knn(base, q, k + 1)
+    assert_knn_matches(base, q, da, ia, rd, ri)
+    a.close()
+    b.close()
