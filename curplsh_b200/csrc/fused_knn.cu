@@ -977,6 +977,7 @@ cudaError_t launch_fused_batch(int form, const FusedItemSpec* specs, const Fused
     if (specs[i].d != specs[0].d) return cudaErrorInvalidValue;
   if (bp.grid == 0) return cudaSuccess;
   const uint32_t smem = make_layout(form, specs[0].d).total;
+  if (smem > 227u * 1024u) return cudaErrorInvalidConfiguration;  // a layout bug, not a caller error
   switch (form) {
     case kFormExact:
       return launch_form_any<kFormExact>(specs, plans, n, bp, status, stats, smem, st);
