@@ -437,9 +437,11 @@ def run_serving(args, world, rank, local):
     recall = None
     for form in (1, 0):
         srv = cb.Server(ix, precision=form, max_inflight=3, max_step_queries=4096, memory_budget=4 << 30)
-        # warm-up
+        # warm-up: a burst, then a few requests spaced out (first-call costs of the paced path)
         sizes = request_sizes(64)
         run_load(srv, sizes, [0.0] * len(sizes))
+        sizes = request_sizes(16)
+        run_load(srv, sizes, [i * 2e-3 for i in range(len(sizes))])
         # saturated throughput: every request queued at once
         sizes = request_sizes(600)
         lat, wall, (qs, outs) = run_load(srv, sizes, [0.0] * len(sizes))

@@ -355,90 +355,6 @@ __device__ __forceinline__ uint64_t warp_select_keep_stream(uint64_t* pool, int 
   return kmax;
 }
 
-// Compact streaming form of the sampled selection (the pool stays in global
-// memory -- it is L1-resident -- and every loop is a runtime loop, so the
-// routine adds little code to the kernel).  Same contract as
-// warp_select_keep_sampled.  Requires n >= 32.
-__device__ __forceinline__ uint32_t warp_stream_count_le(const uint64_t* pool, int n, uint64_t b) {
-  const int lane = threadIdx.x & 31;
-  uint32_t c = 0;
-#pragma unroll 4
-  for (int i = lane; i < n; i += 32) c += pool[i] <= b ? 1u : 0u;
-  return __reduce_add_sync(0xffffffffu, c);
-}
-
-__device__ __noinline__ uint64_t warp_stream_sample_find(const uint64_t* pool, int n, uint64_t smp, uint32_t rank,
-                                                         uint32_t& cnt) {
-  int j = (int)(((long long)rank * 32 + n - 1) / n);
-  j = j < 0 ? 0 : (j > 31 ? 31 : j);
-  uint64_t b = __shfl_sync(0xffffffffu, smp, j);
-  uint32_t c = warp_stream_count_le(pool, n, b);
-  if (c >= rank) {
-    while (j > 0) {
-      const uint64_t b2 = __shfl_sync(0xffffffffu, smp, j - 1);
-      const uint32_t c2 = warp_stream_count_le(pool, n, b2);
-      if (c2 < rank) break;
-      --j;
-      b = b2;
-      c = c2;
-    }
-  } else {
-    while (c < rank && j < 31) {
-      ++j;
-      b = __shfl_sync(0xffffffffu, smp, j);
-      c = warp_stream_count_le(pool, n, b);
-    }
-  }
-  cnt = c;
-  return b;
-}
-
-__device__ __noinline__ uint64_t warp_refresh_pool(uint64_t* pool, int n, int keep, int cap, uint32_t* hist,
-                                                   int& kept, uint64_t& half_key) {
-  const int lane = threadIdx.x & 31;
-  // 32 stratified samples: lane L takes entry L*stride + L % stride
-  const int stride = n / 32;
-  uint64_t smp = pool[lane * stride + (lane % stride)];
-#pragma unroll
-  for (int size = 2; size <= 32; size <<= 1) {
-#pragma unroll
-    for (int st = size >> 1; st > 0; st >>= 1) {
-      const uint64_t other = __shfl_xor_sync(0xffffffffu, smp, st);
-      const bool lower = (lane & st) == 0;
-      const bool asc = (lane & size) == 0;
-      const uint64_t mn = other < smp ? other : smp, mx = other < smp ? smp : other;
-      smp = (lower == asc) ? mn : mx;
-    }
-  }
-  uint32_t c_keep = 0;
-  uint64_t bound = warp_stream_sample_find(pool, n, smp, (uint32_t)keep, c_keep);
-  uint64_t kmax;
-  if (c_keep < (uint32_t)keep || (int)c_keep > cap - pool_sync_tiles(cap, keep) * kBN) {
-    // samples too coarse to free a tile of room: exact radix selection
-    bound = warp_stream_bound(pool, n, kKeyEmpty - 1, (uint32_t)keep, hist);
-    kmax = warp_stream_max_le(pool, n, bound);
-  } else {
-    kmax = bound;  // a sample key, hence the largest key <= bound
-  }
-  uint32_t c_half = 0;
-  half_key = warp_stream_sample_find(pool, n, smp, (uint32_t)((keep + 1) / 2), c_half);
-  if (c_half < (uint32_t)((keep + 1) / 2) || half_key > kmax) half_key = kmax;
-  // in-place stable compaction: every read of a 32-entry round completes
-  // (ballot) before any lane writes, and writes never pass the reads
-  int w = 0;
-  for (int base = 0; base < n; base += 32) {
-    const int i = base + lane;
-    const uint64_t k = (i < n) ? pool[i] : kKeyEmpty;
-    const bool take = k <= bound;
-    const uint32_t bal = __ballot_sync(0xffffffffu, take);
-    if (take) pool[w + __popc(bal & ((1u << lane) - 1u))] = k;
-    w += __popc(bal);
-  }
-  __syncwarp();
-  kept = w;
-  return kmax;
-}
-
 // Dispatch on the pool capacity: registers up to 1024 entries, else streaming.
 __device__ __forceinline__ uint64_t warp_select_keep_any(uint64_t* pool, int n, int keep, int cap, uint32_t* hist,
                                                          int& kept, uint64_t& half_key) {
