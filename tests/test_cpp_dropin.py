@@ -10,12 +10,12 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CUDA = "/usr/local/cuda"
 
 
-def _compile(out):
+def _compile(out, src="test_index_bf.cpp"):
     cxx = shutil.which("g++")
     if not cxx:
         pytest.skip("g++ not available")
     cmd = [cxx, "-std=c++17", "-O2", "-Wall", "-I", os.path.join(ROOT, "include"), "-I", f"{CUDA}/include",
-           os.path.join(ROOT, "tests", "cpp", "test_index_bf.cpp"), "-L", os.path.join(ROOT, "curplsh_b200"),
+           os.path.join(ROOT, "tests", "cpp", src), "-L", os.path.join(ROOT, "curplsh_b200"),
            "-lcurplsh_b200", "-L", f"{CUDA}/lib64", "-lcudart", f"-Wl,-rpath,{os.path.join(ROOT, 'curplsh_b200')}",
            "-o", out]
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -33,3 +33,18 @@ def test_cpp_dropin_runs_reference_pattern(tmp_path):
     r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "cpp drop-in ok" in r.stdout
+
+
+def test_cpp_dataset_header_compiles(tmp_path):
+    _compile(str(tmp_path / "td"), "test_dataset.cpp")
+
+
+@pytest.mark.gpu
+def test_cpp_dataset_search_recall(tmp_path):
+    """include/curplsh/dataset.h: write a SIFT-style directory, load it with
+    DatasetSIFT, search it with IndexBF and evaluate recall (1.0)."""
+    exe = str(tmp_path / "td")
+    _compile(exe, "test_dataset.cpp")
+    r = subprocess.run([exe, str(tmp_path)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "cpp dataset ok" in r.stdout
