@@ -48,3 +48,17 @@ def test_cpp_dataset_search_recall(tmp_path):
     r = subprocess.run([exe, str(tmp_path)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "cpp dataset ok" in r.stdout
+
+
+def test_cpp_device_memory_header_compiles(tmp_path):
+    _compile(str(tmp_path / "tm"), "test_device_memory.cpp")
+
+
+@pytest.mark.gpu
+def test_cpp_device_memory_reservations(tmp_path):
+    """include/curplsh/device_memory.h: stream-ordered reservations, moves, reuse."""
+    exe = str(tmp_path / "tm")
+    _compile(exe, "test_device_memory.cpp")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "cpp device memory ok" in r.stdout
