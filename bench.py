@@ -573,35 +573,53 @@ def main():
     # ---- timed region: device-resident queries, CUDA events on our stream
     peaks = load_peaks()
     flops = 2.0 * Q * n_db * dim
-    launches_per_step = 3  # query prep, fused tensor-core filter, merge + rerank
     timing = {}
+    estimates = {}
     clocks = None
+
+    def timed_searches(ix, steps):
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(steps):
+            ix.search_ex(Q, queries, k, oi, od, stream=stream)
+        ev1.record(stream)
+        ev1.synchronize()
+        return ev0.elapsed_time(ev1) / steps
+
     for form in forms:
         ix = indexes[form]
         for _ in range(args.warmup):
             ix.search_ex(Q, queries, k, oi, od, stream=stream)
         stream.synchronize()
         barrier(world)
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
         sampler = ClockSampler(local) if form == headline else None
         if sampler:
             sampler.__enter__()
-        torch.cuda.synchronize()
-        ev0.record(stream)
-        for _ in range(args.steps):
-            ix.search_ex(Q, queries, k, oi, od, stream=stream)
-        ev1.record(stream)
-        ev1.synchronize()
+        fb0 = ix.fallback_count()
+        ms = timed_searches(ix, args.steps)
+        fb = ix.fallback_count() - fb0
         if sampler:
             sampler.__exit__(None, None, None)
             clocks = sampler.summary()
-        ms = ev0.elapsed_time(ev1) / args.steps
         ms = max_over_ranks(ms, world)
         # per-pass device times (events between passes on the same stream)
         passes = ix.search_profiled(Q, queries, k, oi, od, stream=stream)
         fused_ms = max_over_ranks(passes["fused_ms"], world)
         timing[form] = (ms, fused_ms, passes)
+        rows, step, rank_r = ix.estimate_plan(Q, k, form)
+        est = {"sample_rows": rows, "step": step, "rank": rank_r, "fallback_queries_timed": fb}
+        if rows:
+            # the same searches without the sampled bound estimate, for comparison
+            cb.set_bound_estimate(False)
+            for _ in range(2):
+                ix.search_ex(Q, queries, k, oi, od, stream=stream)
+            est["ms_per_search_without"] = max_over_ranks(timed_searches(ix, max(1, args.steps // 2)), world)
+            cb.set_bound_estimate(True)
+        estimates[form] = est
+    # query prep, [sample pass + estimate merge,] fused tensor-core filter, merge + rerank
+    launches_per_step = 5 if estimates[headline]["sample_rows"] else 3
 
     # ---- end to end through the C ABI: pinned host queries in, host results out
     qh = torch.empty((Q, dim), dtype=torch.float32, pin_memory=True)
@@ -630,7 +648,7 @@ def main():
                 "queries_per_s": Q * world / (f_ms / 1e3), "ms_per_search": f_ms, "fused_ms": f_fused,
                 "fused_tflops": flops / (f_fused / 1e3) / 1e12,
                 "roofline_frac": flops / (f_fused / 1e3) / 1e12 / p_form,
-                "peak_basis_tflops": p_form, **form_results.get(name, {}),
+                "peak_basis_tflops": p_form, "bound_estimate": estimates[form], **form_results.get(name, {}),
             }
         achieved = flops / (fused_ms / 1e3) / 1e12
         rec = form_results.get(FORMS[headline], {}).get("recall_at_k")
@@ -653,9 +671,13 @@ def main():
             "e2e": {"value": Q * world / (e2e / 1e3), "unit": "queries/s", "ms_per_step": e2e,
                     "h2d_bytes_per_step": Q * dim * 4, "d2h_bytes_per_step": Q * k * 8},
             "gpu_launches": launches_per_step * args.steps,
-            "launches_per_step": {"prep_rows_kernel": 1, "fused_knn_kernel": 1, "merge_rerank_kernel": 1},
+            "launches_per_step": ({"prep_rows_kernel": 1, "fused_knn_kernel": 2, "merge_rerank_kernel": 2}
+                                  if launches_per_step == 5 else
+                                  {"prep_rows_kernel": 1, "fused_knn_kernel": 1, "merge_rerank_kernel": 1}),
             "clocks": clocks,
             "passes_ms": {k_: v for k_, v in passes.items()},
+            "passes_note": "prep_ms includes the sample pass and estimate merge when bound_estimate.sample_rows > 0; "
+                           "fused_ms is the full-database fused launch the roofline is taken on",
         }
         print(json.dumps(line), flush=True)
     for ix in indexes.values():

@@ -129,6 +129,11 @@ def _load():
         "curplsh_server_get_stats": (i32, [vp, ctypes.POINTER(_ServerStats)]),
         "curplsh_server_destroy": (i32, [vp]),
         "curplsh_merge_shard_results": (i32, [i64, i32, i32, f32p, i32p, vp, i32p, f32p, vp]),
+        "curplsh_set_bound_estimate": (i32, [i32]),
+        "curplsh_get_bound_estimate": (i32, [ctypes.POINTER(ctypes.c_int)]),
+        "curplsh_index_estimate_plan": (i32, [vp, i64, i32, i32, i32, ctypes.POINTER(ctypes.c_int),
+                                              ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+        "curplsh_index_get_fallback_count": (i32, [vp, ctypes.POINTER(ctypes.c_int64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -153,6 +158,8 @@ EXPORTED_SYMBOLS = (
     "curplsh_batch_get_info", "curplsh_batch_destroy", "curplsh_tuning_set", "curplsh_tuning_get",
     "curplsh_tuning_clear", "curplsh_server_config_init", "curplsh_server_create", "curplsh_server_submit",
     "curplsh_server_wait", "curplsh_server_get_stats", "curplsh_server_destroy", "curplsh_merge_shard_results",
+    "curplsh_set_bound_estimate", "curplsh_get_bound_estimate", "curplsh_index_estimate_plan",
+    "curplsh_index_get_fallback_count",
 )
 
 
@@ -355,6 +362,22 @@ class IndexBF:
     def getResources(self) -> DeviceResources:
         return self._res
 
+    def estimate_plan(self, num_queries: int, k: int, precision: int = -1, rerank_factor: int = -1):
+        """(sample_rows, step, rank) of the sampled bound estimate a search of this
+        shape would use (rank among the sample_rows / 128 block minima);
+        sample_rows == 0 when it uses none."""
+        a, b, c = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+        _check(_lib.curplsh_index_estimate_plan(self._h, int(num_queries), int(k), int(precision),
+                                                int(rerank_factor), ctypes.byref(a), ctypes.byref(b),
+                                                ctypes.byref(c)))
+        return a.value, b.value, c.value
+
+    def fallback_count(self) -> int:
+        """Queries searched again after their estimated bound failed (since creation)."""
+        v = ctypes.c_int64()
+        _check(_lib.curplsh_index_get_fallback_count(self._h, ctypes.byref(v)))
+        return v.value
+
     # -- convenience forms
     def add_array(self, data) -> None:
         self.add(int(data.shape[0]), data)
@@ -461,6 +484,17 @@ def tuning_get(precision: int, dim: int, k: int, num_queries: int):
 
 def tuning_clear() -> None:
     _check(_lib.curplsh_tuning_clear())
+
+
+def set_bound_estimate(enabled: bool) -> None:
+    """Process-wide switch of the sampled bound estimate (speed only; results are identical)."""
+    _check(_lib.curplsh_set_bound_estimate(1 if enabled else 0))
+
+
+def get_bound_estimate() -> bool:
+    v = ctypes.c_int(0)
+    _check(_lib.curplsh_get_bound_estimate(ctypes.byref(v)))
+    return bool(v.value)
 
 
 class Server:

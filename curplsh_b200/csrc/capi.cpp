@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cfloat>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -130,11 +131,11 @@ struct PinnedBuf {
 struct Carve {
   char* base;
   size_t off = 0;
-  explicit Carve(void* b) : base(static_cast<char*>(b)) {}
+  explicit Carve(void* b) : base(static_cast<char*>(b)) {}  // null base: only sizes the carve
   template <class T>
   T* take(size_t count) {
     off = (size_t)round_up((long long)off, 256);
-    T* p = reinterpret_cast<T*>(base + off);
+    T* p = base ? reinterpret_cast<T*>(base + off) : nullptr;
     off += count * sizeof(T);
     return p;
   }
@@ -195,8 +196,13 @@ int init_device(curplsh_resources* r, int device, DevRes** out) {
 namespace {
 struct StreamWorkspace {
   DevBuf dev;      // query operands, pools, staging
+  DevBuf fb;       // re-search of the queries an estimated bound failed
   PinnedBuf host;  // status read-back
 };
+
+// Library-wide switch of the sampled bound estimate (results are identical
+// either way; it only changes speed).
+std::atomic<int> g_bound_estimate{1};
 }  // namespace
 
 struct curplsh_index {
@@ -220,6 +226,7 @@ struct curplsh_index {
   bool bf16_exact = false;        // every stored value is exactly a BF16 value (rerank reads xh)
   long long generation = 0;       // bumped whenever the prepared database changes (add, reset)
   cudaEvent_t order_ev = nullptr; // orders default-stream searches after the legacy stream
+  std::atomic<long long> fallback_queries{0};  // queries re-searched after an estimate failed
   std::map<cudaStream_t, std::unique_ptr<StreamWorkspace>> ws;
 
   void free_db() {
@@ -295,10 +302,166 @@ struct Timing {
   }
 };
 
+// ---- sampled bound estimate
+// Without a bound, a candidate pool admits every row until it holds k' keys
+// and then tightens as it sees more rows: about k'(1 + ln(rows / k')) rows
+// per pool survive the filter, and appending and selecting survivors is most
+// of the fused pass's time.  A short first pass over a strided sample of the
+// database (rows 0, s, 2s, ...; same form) records, per query, the smallest
+// coarse distance of every 128-row block of the sample (no pools, no
+// survivors), and the j-th smallest of those B block minima becomes the
+// starting bound E of every pool of the full pass.  If a fraction p of the
+// database lies under a distance x, a block's minimum is under x with
+// probability q(p) = 1 - (1 - p)^128, so the number of block minima under the
+// query's k'-th distance is Binomial(B, q(k'/N)); j is the smallest rank whose
+// upper tail is <= 1e-6, and E admits about N * (1 - (1 - j/B)^(1/128)) rows.
+// E is a guess, not a bound; the merge pass checks it exactly: when at least
+// k' candidates lie under the final bound, the k' nearest rows are among them
+// (see merge_rerank.cu), otherwise the query is searched again without an
+// estimate.  Results never depend on E.
+struct EstimatePlan {
+  bool on = false;
+  int rows = 0;    // sample rows (a multiple of 256)
+  int step = 1;    // sample row j is database row j * step
+  int blocks = 0;  // B = rows / 128 block minima per query
+  int j = 0;       // rank of the estimate among the block minima
+  FusedPlan plan;
+};
+
+// P(X >= j) for X ~ Binomial(n, q).
+double binomial_tail(int n, double q, int j) {
+  if (j <= 0) return 1.0;
+  if (j > n) return 0.0;
+  const double lq = std::log(q), l1q = std::log1p(-q);
+  double t = 0.0;
+  for (int i = j; i <= n; ++i) {
+    const double term =
+        std::exp(std::lgamma(n + 1.0) - std::lgamma(i + 1.0) - std::lgamma(n - i + 1.0) + i * lq + (n - i) * l1q);
+    t += term;
+    if (term < t * 1e-12) break;
+  }
+  return t;
+}
+
+constexpr double kEstimateMu = 12.0;        // expected sample rows among a query's k' nearest
+constexpr double kEstimateFailure = 1e-6;   // per-query failure probability for a uniform sample
+constexpr int kEstimateBlockRows = kHalfN;  // rows per block minimum (one epilogue warp's half tile)
+
+EstimatePlan plan_estimate(int nq, long long n, int kp, int num_sms) {
+  EstimatePlan e;
+  if (!g_bound_estimate.load(std::memory_order_relaxed) || nq < 1 || kp < 1) return e;
+  if (n < (1LL << 16) || n < 64LL * kp) return e;  // a short search gains too little
+  const long long T = (n + kBN - 1) / kBN;
+  const long long tiles = (long long)std::ceil(kEstimateMu * (double)n / kp / kBN);
+  if (tiles * 10 > T) return e;  // the sample pass must cost at most a tenth of the full pass
+  e.rows = (int)(tiles * kBN);
+  e.step = (int)(n / e.rows);  // >= 10; rows j * step < n for every j < rows
+  e.blocks = e.rows / kEstimateBlockRows;
+  const double q0 = -std::expm1(kEstimateBlockRows * std::log1p(-(double)kp / (double)n));
+  int j = 1;
+  while (j < e.blocks && binomial_tail(e.blocks, q0, j) > kEstimateFailure) ++j;
+  if (2 * j > e.blocks) return e;
+  e.j = j;
+  plan_fused(nq, e.rows, num_sms, &e.plan);
+  e.on = true;
+  return e;
+}
+
+// Sizes and carve of one search's device workspace (search_device and
+// search_workspace_bytes use the same layout).
+struct SearchShape {
+  int kp = 0, P = 0;
+  FusedPlan plan;
+  long long nq_pad = 0;
+  size_t pool_lists = 0;
+  EstimatePlan est;
+};
+
+SearchShape search_shape(const curplsh_index* ix, int nq, int k, int form, int rerank_factor, bool allow_est) {
+  SearchShape sh;
+  sh.kp = kprime_for(form, k, rerank_factor, ix->n);
+  const TuneParams tp = tune_lookup(form, ix->dim, k, nq);
+  sh.P = pool_capacity(sh.kp, tp.headroom);
+  plan_fused(nq, (int)ix->n, ix->dres->num_sms, &sh.plan, default_split_q4(tp, sh.P));
+  sh.nq_pad = round_up(nq, kBM);
+  sh.pool_lists = (size_t)sh.plan.num_qblocks * kBM * sh.plan.units_per_block;
+  if (allow_est) sh.est = plan_estimate(nq, ix->n, sh.kp, ix->dres->num_sms);
+  return sh;
+}
+
+struct SearchBufs {
+  __nv_bfloat16 *qh = nullptr, *ql = nullptr;
+  uint8_t* q8 = nullptr;
+  float *qn = nullptr, *qs = nullptr;
+  uint32_t* qbound = nullptr;   // [nq_pad] bounds of the full pass
+  float* minima = nullptr;      // [nq_pad][B] block minima of the sample pass
+  int* fail = nullptr;          // [1 + nq]: count, then query indices
+  int* counts = nullptr;
+  uint64_t* pools = nullptr;
+};
+
+size_t carve_search(Carve& c, const curplsh_index* ix, const SearchShape& sh, int nq, int form, SearchBufs* b) {
+  b->qh = c.take<__nv_bfloat16>((size_t)sh.nq_pad * ix->ld16);
+  if (form == kFormExact) b->ql = c.take<__nv_bfloat16>((size_t)sh.nq_pad * ix->ld16);
+  if (form == kFormFP8) b->q8 = c.take<uint8_t>((size_t)sh.nq_pad * ix->ld8);
+  b->qn = c.take<float>(sh.nq_pad);
+  b->qs = c.take<float>(sh.nq_pad);
+  b->qbound = c.take<uint32_t>(sh.nq_pad);
+  if (sh.est.on) {
+    b->minima = c.take<float>((size_t)sh.nq_pad * sh.est.blocks);
+    b->fail = c.take<int>(1 + (size_t)nq);
+  }
+  b->counts = c.take<int>(sh.pool_lists);
+  b->pools = c.take<uint64_t>(sh.pool_lists * (size_t)sh.P);
+  return (size_t)round_up((long long)c.off, 256);
+}
+
+#ifdef CURPLSH_FUSED_STATS
+// Instrumented builds: per-role cycle counters of a fused launch, printed to stderr.
+cudaError_t fused_stats_begin(FusedLaunch* f, cudaStream_t st) {
+  static unsigned long long* stats = nullptr;
+  if (!stats) {
+    cudaError_t e = cudaMalloc(&stats, kStatCount * sizeof(unsigned long long));
+    if (e != cudaSuccess) return e;
+  }
+  f->stats = stats;
+  return cudaMemsetAsync(stats, 0, kStatCount * sizeof(unsigned long long), st);
+}
+
+cudaError_t fused_stats_print(const char* label, const FusedLaunch& f, cudaStream_t st) {
+  unsigned long long h[kStatCount];
+  cudaError_t e = cudaMemcpyAsync(h, f.stats, sizeof(h), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return e;
+  const FusedPlan& plan = f.plan;
+  const double ctas = (double)plan.grid;
+  fprintf(stderr,
+          "[fused-stats %s] grid %d kp %d P %d | per CTA (Mcycles): total %.2f prod_wait_empty %.2f mma_wait_full "
+          "%.2f mma_wait_acc %.2f | per epi warp: wait_acc %.2f filter %.2f refresh %.2f | refreshes %llu survivors "
+          "%llu\n",
+          label, plan.grid, f.kprime, f.pool_cap, h[kStatCtaCycles] / ctas / 1e6, h[kStatProducerWaitEmpty] / ctas / 1e6,
+          h[kStatMmaWaitFull] / ctas / 1e6, h[kStatMmaWaitAccEmpty] / ctas / 1e6, h[kStatEpiWaitAccFull] / ctas / 8 / 1e6,
+          h[kStatEpiFilter] / ctas / 8 / 1e6, h[kStatEpiRefresh] / ctas / 8 / 1e6, h[kStatRefreshes],
+          h[kStatSurvivors]);
+  fprintf(stderr,
+          "[fused-stats2 %s] radix passes/refresh %.2f | slow chunks %llu (%.1f%% of warp-chunks) | loop iters/slow "
+          "chunk %.2f | tmem Mcycles/warp %.2f | pair barriers Mcycles/warp %.2f\n",
+          label, h[kStatRefreshes] ? (double)h[kStatRadixPasses] / h[kStatRefreshes] : 0.0, h[kStatSlowChunks],
+          100.0 * h[kStatSlowChunks] / (ctas * 8 * (double)plan.work_per_cta * 4),
+          h[kStatSlowChunks] ? (double)h[kStatLoopIters] / h[kStatSlowChunks] : 0.0,
+          h[kStatTmemCycles] / ctas / 8 / 1e6, h[kStatPairBarrier] / ctas / 8 / 1e6);
+  return cudaSuccess;
+}
+#endif
+
 // The search proper.  Device-side inputs/outputs; `st` orders everything.
+// With `allow_est` a sampled bound estimate may be used; then *fail_out
+// points at the device list of queries it failed ([0] count, then indices),
+// which the caller must search again (else *fail_out is null).
 int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form, int rerank_factor, int* out_idx,
-                  float* out_dist, cudaStream_t st, StreamWorkspace& w, char* extra_base, Timing* tm) {
+                  float* out_dist, cudaStream_t st, char* extra_base, Timing* tm, bool allow_est, int** fail_out) {
   const int d = ix->dim;
+  *fail_out = nullptr;
   if (ix->n == 0) {
     CUDA_TRY(launch_fill_results(out_idx, out_dist, (long long)nq * k, st));
     return CURPLSH_OK;
@@ -307,30 +470,17 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
     int rc = build_fp8(ix, st);
     if (rc) return rc;
   }
-  const int kp = kprime_for(form, k, rerank_factor, ix->n);
-  const TuneParams tp = tune_lookup(form, d, k, nq);
-  const int P = pool_capacity(kp, tp.headroom);
-  FusedPlan plan;
-  plan_fused(nq, (int)ix->n, ix->dres->num_sms, &plan, default_split_q4(tp, P));
-  const long long nq_pad = round_up(nq, kBM);
-  const size_t pool_lists = (size_t)plan.num_qblocks * kBM * plan.units_per_block;
-
+  const SearchShape sh = search_shape(ix, nq, k, form, rerank_factor, allow_est);
+  const int kp = sh.kp, P = sh.P;
+  const FusedPlan& plan = sh.plan;
+  const long long nq_pad = sh.nq_pad;
   Carve c(extra_base);
-  __nv_bfloat16* qh = c.take<__nv_bfloat16>((size_t)nq_pad * ix->ld16);
-  __nv_bfloat16* ql = form == kFormExact ? c.take<__nv_bfloat16>((size_t)nq_pad * ix->ld16) : nullptr;
-  uint8_t* q8 = form == kFormFP8 ? c.take<uint8_t>((size_t)nq_pad * ix->ld8) : nullptr;
-  float* qn = c.take<float>(nq_pad);
-  float* qs = c.take<float>(nq_pad);
-  uint32_t* qbound = c.take<uint32_t>(3 * nq_pad);  // [nq_pad] k'-th bounds, then [nq_pad][2] half bounds
-  int* counts = c.take<int>(pool_lists);
-  uint64_t* pools = c.take<uint64_t>(pool_lists * (size_t)P);
-  (void)w;
+  SearchBufs b;
+  carve_search(c, ix, sh, nq, form, &b);
 
   tm->rec(1, st);
-  CUDA_TRY(launch_prep_rows(q_dev, d, nq, nq_pad, d, qn, 0.f, form == kFormFP8 ? nullptr : qh, ql, ix->ld16,
-                            q8, qs, ix->ld8, st, form == kFormFP8 ? kAugNone : kAugQuery));
-  CUDA_TRY(cudaMemsetAsync(qbound, 0xFF, (size_t)3 * nq_pad * sizeof(uint32_t), st));
-  tm->rec(2, st);
+  CUDA_TRY(launch_prep_rows(q_dev, d, nq, nq_pad, d, b.qn, 0.f, form == kFormFP8 ? nullptr : b.qh, b.ql, ix->ld16,
+                            b.q8, b.qs, ix->ld8, st, form == kFormFP8 ? kAugNone : kAugQuery));
   FusedLaunch f{};
   f.nq = nq;
   f.nb = (int)ix->n;
@@ -342,51 +492,50 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
   f.nb_pad = ix->n_pad;
   f.ld16 = ix->ld16;
   f.ld8 = ix->ld8;
-  f.qh = qh;
-  f.ql = ql;
-  f.q8 = q8;
-  f.qn = qn;
-  f.qs = qs;
+  f.qh = b.qh;
+  f.ql = b.ql;
+  f.q8 = b.q8;
+  f.qn = b.qn;
+  f.qs = b.qs;
   f.xh = ix->xh;
   f.xl = ix->xl;
   f.x8 = ix->x8;
   f.xn = ix->xn;
   f.xs = ix->xs;
-  f.pools = pools;
-  f.pool_counts = counts;
-  f.q_bound = qbound;
-  f.q_bound_half = qbound + nq_pad;
+  f.pools = b.pools;
+  f.pool_counts = b.counts;
+  f.q_bound = b.qbound;
   f.status = ix->status;
   f.plan = plan;
+  if (sh.est.on) {
+    // sample pass over rows 0, step, 2 step, ...: block minima, no pools
+    FusedLaunch e = f;
+    e.nb = sh.est.rows;
+    e.nb_pad = sh.est.rows;
+    e.db_step = sh.est.step;
+    e.kprime = 1;
+    e.minima = b.minima;
+    e.plan = sh.est.plan;
+    CUDA_TRY(cudaMemsetAsync(b.fail, 0, sizeof(int), st));
 #ifdef CURPLSH_FUSED_STATS
-  // instrumented builds: per-role cycle counters of the fused pass, printed to stderr
-  static unsigned long long* stats = nullptr;
-  if (!stats) CUDA_TRY(cudaMalloc(&stats, kStatCount * sizeof(unsigned long long)));
-  CUDA_TRY(cudaMemsetAsync(stats, 0, kStatCount * sizeof(unsigned long long), st));
-  f.stats = stats;
+    CUDA_TRY(fused_stats_begin(&e, st));
+#endif
+    CUDA_TRY(launch_fused(e, st));
+#ifdef CURPLSH_FUSED_STATS
+    CUDA_TRY(fused_stats_print("sample", e, st));
+#endif
+    // the j-th smallest block minimum of every query becomes its starting bound
+    CUDA_TRY(launch_estimate_select(b.minima, sh.est.blocks, nq, sh.est.j, b.qbound, st));
+  } else {
+    CUDA_TRY(cudaMemsetAsync(b.qbound, 0xFF, (size_t)nq_pad * sizeof(uint32_t), st));
+  }
+  tm->rec(2, st);
+#ifdef CURPLSH_FUSED_STATS
+  CUDA_TRY(fused_stats_begin(&f, st));
 #endif
   CUDA_TRY(launch_fused(f, st));
 #ifdef CURPLSH_FUSED_STATS
-  {
-    unsigned long long h[kStatCount];
-    CUDA_TRY(cudaMemcpyAsync(h, stats, sizeof(h), cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
-    const double ctas = (double)plan.grid;
-    fprintf(stderr,
-            "[fused-stats] grid %d kp %d P %d | per CTA (Mcycles): total %.2f prod_wait_empty %.2f mma_wait_full %.2f "
-            "mma_wait_acc %.2f | per epi warp: wait_acc %.2f filter %.2f refresh %.2f | refreshes %llu survivors %llu\n",
-            plan.grid, kp, P, h[kStatCtaCycles] / ctas / 1e6, h[kStatProducerWaitEmpty] / ctas / 1e6,
-            h[kStatMmaWaitFull] / ctas / 1e6, h[kStatMmaWaitAccEmpty] / ctas / 1e6,
-            h[kStatEpiWaitAccFull] / ctas / 8 / 1e6, h[kStatEpiFilter] / ctas / 8 / 1e6,
-            h[kStatEpiRefresh] / ctas / 8 / 1e6, h[kStatRefreshes], h[kStatSurvivors]);
-    fprintf(stderr,
-            "[fused-stats2] radix passes/refresh %.2f | slow chunks %llu (%.1f%% of warp-chunks) | loop iters/slow "
-            "chunk %.2f | tmem Mcycles/warp %.2f | pair barriers Mcycles/warp %.2f\n",
-            h[kStatRefreshes] ? (double)h[kStatRadixPasses] / h[kStatRefreshes] : 0.0, h[kStatSlowChunks],
-            100.0 * h[kStatSlowChunks] / (ctas * 8 * (double)plan.work_per_cta * 4),
-            h[kStatSlowChunks] ? (double)h[kStatLoopIters] / h[kStatSlowChunks] : 0.0,
-            h[kStatTmemCycles] / ctas / 8 / 1e6, h[kStatPairBarrier] / ctas / 8 / 1e6);
-  }
+  CUDA_TRY(fused_stats_print("full", f, st));
 #endif
   tm->rec(3, st);
   MergeLaunch m{};
@@ -397,10 +546,13 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
   m.kprime = kp;
   m.pool_cap = P;
   m.plan = plan;
-  m.pools = pools;
-  m.pool_counts = counts;
-  m.q_bound = qbound;
-  m.q_bound_half = qbound + nq_pad;
+  m.pools = b.pools;
+  m.pool_counts = b.counts;
+  m.q_bound = b.qbound;
+  if (sh.est.on) {
+    m.fail_count = b.fail;
+    m.fail_list = b.fail + 1;
+  }
   m.queries = q_dev;
   m.db = ix->x32;
   m.ld_db = d;
@@ -413,29 +565,46 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
   m.status = ix->status;
   CUDA_TRY(launch_merge_rerank(m, st));
   tm->rec(4, st);
+  if (sh.est.on) *fail_out = b.fail;
   return CURPLSH_OK;
 }
 
-size_t search_workspace_bytes(const curplsh_index* ix, int nq, int k, int form, int rerank_factor) {
+size_t search_workspace_bytes(const curplsh_index* ix, int nq, int k, int form, int rerank_factor,
+                              bool allow_est) {
   if (ix->n == 0) return 0;
-  const int kp = kprime_for(form, k, rerank_factor, ix->n);
-  const TuneParams tp = tune_lookup(form, ix->dim, k, nq);
-  const int P = pool_capacity(kp, tp.headroom);
-  FusedPlan plan;
-  plan_fused(nq, (int)ix->n, ix->dres->num_sms, &plan, default_split_q4(tp, P));
-  const long long nq_pad = round_up(nq, kBM);
-  const size_t pool_lists = (size_t)plan.num_qblocks * kBM * plan.units_per_block;
-  size_t b = 0;
-  auto add = [&](size_t bytes) { b = (size_t)round_up((long long)b, 256) + bytes; };
-  add((size_t)nq_pad * ix->ld16 * 2);
-  if (form == kFormExact) add((size_t)nq_pad * ix->ld16 * 2);
-  if (form == kFormFP8) add((size_t)nq_pad * ix->ld8);
-  add(nq_pad * 4);
-  add(nq_pad * 4);
-  add(nq_pad * 12);
-  add(pool_lists * 4);
-  add(pool_lists * (size_t)P * 8);
-  return (size_t)round_up((long long)b, 256) + 256;
+  const SearchShape sh = search_shape(ix, nq, k, form, rerank_factor, allow_est);
+  Carve c(nullptr);
+  SearchBufs b;
+  return carve_search(c, ix, sh, nq, form, &b) + 256;
+}
+
+// Searches again, without an estimate, the `nf` queries listed at fail_dev + 1
+// (device) and writes their results into the full result arrays.
+int search_failed(curplsh_index* ix, int nf, const int* fail_dev, const float* q_dev, int k, int form,
+                  int rerank_factor, int* out_idx, float* out_dist, cudaStream_t st, StreamWorkspace& w) {
+  const int d = ix->dim;
+  const size_t qbytes = (size_t)round_up((long long)nf * d * sizeof(float), 256);
+  const size_t obytes = (size_t)round_up((long long)nf * k * (sizeof(int) + sizeof(float)), 256);
+  const size_t core = search_workspace_bytes(ix, nf, k, form, rerank_factor, false);
+  cudaError_t e = w.fb.ensure(qbytes + obytes + core);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(CURPLSH_ERR_OOM, "re-search workspace of %zu bytes: %s", qbytes + obytes + core,
+                     cudaGetErrorString(e));
+  }
+  char* base = static_cast<char*>(w.fb.ptr);
+  float* qf = reinterpret_cast<float*>(base);
+  int* oif = reinterpret_cast<int*>(base + qbytes);
+  float* odf = reinterpret_cast<float*>(base + qbytes + (size_t)nf * k * sizeof(int));
+  CUDA_TRY(launch_gather_rows(q_dev, d, fail_dev + 1, nf, qf, st));
+  Timing none;
+  int* again = nullptr;
+  int rc = search_device(ix, nf, qf, k, form, rerank_factor, oif, odf, st, base + qbytes + obytes, &none, false,
+                         &again);
+  if (rc) return rc;
+  CUDA_TRY(launch_scatter_results(oif, odf, fail_dev + 1, nf, k, out_idx, out_dist, st));
+  ix->fallback_queries.fetch_add(nf, std::memory_order_relaxed);
+  return CURPLSH_OK;
 }
 
 int do_search(curplsh_index* ix, int64_t num, const float* queries, int k, int precision, int rerank_factor,
@@ -464,12 +633,15 @@ int do_search(curplsh_index* ix, int64_t num, const float* queries, int k, int p
   const bool q_dev = pointer_device(queries) == dev;
   const bool i_dev = pointer_device(indices) == dev;
   const bool d_dev = pointer_device(distances) == dev;
-  const bool sync = force_sync || !(q_dev && i_dev && d_dev);
+  // A search that starts from an estimated bound checks it on the host (a
+  // failed query is searched again), so it always returns synchronised.
+  const bool est = ix->n > 0 && plan_estimate(nq, ix->n, kprime_for(form, k, rf, ix->n), ix->dres->num_sms).on;
+  const bool sync = force_sync || est || !(q_dev && i_dev && d_dev);
 
   auto& slot = ix->ws[st];
   if (!slot) slot.reset(new StreamWorkspace());
   StreamWorkspace& w = *slot;
-  const size_t core = search_workspace_bytes(ix, nq, k, form, rf);
+  const size_t core = search_workspace_bytes(ix, nq, k, form, rf, true);
   const size_t qbytes = q_dev ? 0 : (size_t)nq * ix->dim * sizeof(float);
   const size_t obytes = (i_dev && d_dev) ? 0 : (size_t)nq * k * (sizeof(int) + sizeof(float));
   const size_t total = (size_t)round_up((long long)qbytes, 256) + (size_t)round_up((long long)obytes, 256) + core;
@@ -501,17 +673,38 @@ int do_search(curplsh_index* ix, int64_t num, const float* queries, int k, int p
   tm.rec(0, st);
   if (!q_dev)
     CUDA_TRY(cudaMemcpyAsync(const_cast<float*>(qd), queries, qbytes, cudaMemcpyDefault, st));
-  int rc = search_device(ix, nq, qd, k, form, rf, oi, od, st, w, base + off, &tm);
+  int* fail = nullptr;
+  int rc = search_device(ix, nq, qd, k, form, rf, oi, od, st, base + off, &tm, true, &fail);
   if (rc) return rc;
-  if (!(i_dev && d_dev)) {
-    CUDA_TRY(cudaMemcpyAsync(indices, oi, (size_t)nq * k * sizeof(int), cudaMemcpyDefault, st));
-    CUDA_TRY(cudaMemcpyAsync(distances, od, (size_t)nq * k * sizeof(float), cudaMemcpyDefault, st));
-  }
+  auto copy_out = [&]() -> int {
+    if (!(i_dev && d_dev)) {
+      CUDA_TRY(cudaMemcpyAsync(indices, oi, (size_t)nq * k * sizeof(int), cudaMemcpyDefault, st));
+      CUDA_TRY(cudaMemcpyAsync(distances, od, (size_t)nq * k * sizeof(float), cudaMemcpyDefault, st));
+    }
+    return CURPLSH_OK;
+  };
+  rc = copy_out();
+  if (rc) return rc;
   if (pass_ms) tm.rec(4, st);  // whole-search end (after copies)
   if (sync) {
-    CUDA_TRY(cudaMemcpyAsync(w.host.ptr, ix->status, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    uint32_t* hw = static_cast<uint32_t*>(w.host.ptr);
+    hw[1] = 0;
+    CUDA_TRY(cudaMemcpyAsync(hw, ix->status, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    if (fail) CUDA_TRY(cudaMemcpyAsync(hw + 1, fail, sizeof(int), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
-    const uint32_t s = *static_cast<uint32_t*>(w.host.ptr);
+    uint32_t s = hw[0];
+    const int nf = (int)hw[1];
+    if (!s && nf > 0) {
+      // queries whose estimated bound was too small: search them again
+      rc = search_failed(ix, nf, fail, qd, k, form, rf, oi, od, st, w);
+      if (rc) return rc;
+      rc = copy_out();
+      if (rc) return rc;
+      if (pass_ms) tm.rec(4, st);
+      CUDA_TRY(cudaMemcpyAsync(hw, ix->status, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+      CUDA_TRY(cudaStreamSynchronize(st));
+      s = hw[0];
+    }
     if (s) {
       cudaMemsetAsync(ix->status, 0, sizeof(uint32_t), st);
       cudaStreamSynchronize(st);
@@ -858,6 +1051,45 @@ int curplsh_index_get_num_data(const curplsh_index* ix, int64_t* out) {
   *out = ix->n;
   return CURPLSH_OK;
 }
+int curplsh_set_bound_estimate(int enabled) {
+  g_bound_estimate.store(enabled ? 1 : 0, std::memory_order_relaxed);
+  return CURPLSH_OK;
+}
+
+int curplsh_get_bound_estimate(int* enabled) {
+  if (!enabled) return set_error(CURPLSH_ERR_INVALID_ARG, "null argument");
+  *enabled = g_bound_estimate.load(std::memory_order_relaxed);
+  return CURPLSH_OK;
+}
+
+int curplsh_index_estimate_plan(curplsh_index* ix, int64_t num, int k, int precision, int rerank_factor,
+                                int* sample_rows, int* step, int* rank) {
+  if (!ix || !sample_rows || !step || !rank) return set_error(CURPLSH_ERR_INVALID_ARG, "null argument");
+  if (k < 1 || k > 1024 || num < 0 || num > (int64_t)1 << 30)
+    return set_error(CURPLSH_ERR_INVALID_ARG, "bad k or number of queries");
+  const int form = precision < 0 ? ix->cfg.precision : precision;
+  if (form < 0 || form > 2) return set_error(CURPLSH_ERR_INVALID_ARG, "unknown precision %d", precision);
+  const int rf = rerank_factor > 0 ? rerank_factor : ix->cfg.rerank_factor;
+  std::lock_guard<std::mutex> lk(ix->mu);
+  *sample_rows = 0;
+  *step = 1;
+  *rank = 0;
+  if (ix->n == 0) return CURPLSH_OK;
+  const EstimatePlan e = plan_estimate((int)num, ix->n, kprime_for(form, k, rf, ix->n), ix->dres->num_sms);
+  if (e.on) {
+    *sample_rows = e.rows;
+    *step = e.step;
+    *rank = e.j;
+  }
+  return CURPLSH_OK;
+}
+
+int curplsh_index_get_fallback_count(curplsh_index* ix, int64_t* count) {
+  if (!ix || !count) return set_error(CURPLSH_ERR_INVALID_ARG, "null argument");
+  *count = ix->fallback_queries.load(std::memory_order_relaxed);
+  return CURPLSH_OK;
+}
+
 int curplsh_index_get_device(const curplsh_index* ix, int* out) {
   if (!ix || !out) return set_error(CURPLSH_ERR_INVALID_ARG, "null argument");
   *out = ix->cfg.device;

@@ -98,10 +98,14 @@ struct FusedItem {
   const float* db_scale;   // [nb_pad] fp8 per-vector scales (FP8 form)
   const float* q_norms;    // [nq_pad]
   const float* q_scale;    // [nq_pad] (FP8 form)
-  uint64_t* pools;         // [G_i*128][U_i][2][pool_cap]
-  int* pool_counts;        // [G_i*128][U_i][2]
-  uint32_t* q_bound;       // [nq_pad] shared per-query bound (ordered bits), init kOrdInf
-  uint32_t* q_bound_half;  // [nq_pad][2] per-query, per-half (k'/2)-th bounds, init kOrdInf
+  uint64_t* pools;         // [G_i*128][U_i][pool_cap]
+  int* pool_counts;        // [G_i*128][U_i]
+  uint32_t* q_bound;       // [nq_pad] shared per-query bound (ordered bits), init kOrdInf or an estimate
+  int db_step;             // database row j of this item is stored row j * db_step (>= 1)
+  int reserved;
+  // Non-null: block-minimum mode (no pools): minima[q * 2 * num_tiles + 2 * t + h]
+  // gets the smallest key distance of query q over rows [256 t + 128 h, +128).
+  float* minima;
 };
 
 // Tensor maps of one item, in this order.

@@ -584,7 +584,8 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
         if (Tr::kFP8) {
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
-            const int c = tphys * kBN + g * kHalfN + lane + 32 * i;  // < nb_pad: rows are padded to whole tiles
+            // < nb_pad: rows are padded to whole tiles (a strided sample has no padding)
+            const size_t c = (size_t)(tphys * kBN + g * kHalfN + lane + 32 * i) * (size_t)p.db_step;
             pxn[i] = __ldg(p.db_norms + c);
             psx[i] = __ldg(p.db_scale + c);
           }
@@ -598,6 +599,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
         STAT_BEGIN(tfl);
         tc_fence_after();
         const int colh = tphys * kBN + g * kHalfN;
+        float bmin = 3.402823466e38f;  // block-minimum mode: smallest distance of this half tile
         float* colv = reinterpret_cast<float*>(hist);  // [128] norms, then [128] scales
         if (Tr::kFP8) {
           __syncwarp();
@@ -642,6 +644,19 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
               fma2_f32(dst[o + 2], dst[o + 3], p2, p3, m2s, m2s, xn.z, xn.w);
             }
           }
+          if (p.minima) {
+            // block-minimum mode: no survivors, only the half tile's smallest
+            // distance (columns past nb excluded)
+            const int lim = p.nb - col0;
+            float m0 = 3.402823466e38f, m1 = 3.402823466e38f;
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+              if (j < lim) m0 = fminf(m0, da[j]);
+              if (32 + j < lim) m1 = fminf(m1, db[j]);
+            }
+            bmin = fminf(bmin, fminf(m0, m1));
+            continue;
+          }
           // survivor masks, each OR-combined in four independent partial masks
           uint32_t ma, mb;
           {
@@ -680,6 +695,20 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
               const int c = __popc(ma) + __popc(mb);
               if (c) n = atomicAdd(&cnt_s[row], c);
             }
+            if ((ma & mb) == ~0u) {
+              // every column survives (a pool with no bound yet): append all
+              // 64 keys in column order, no extraction
+#pragma unroll
+              for (int j = 0; j < 32; ++j)
+                if (n + j < P) pool[n + j] = make_key(Tr::kFolded ? da[j] : da[j] + qn, (uint32_t)(col0 + j));
+#pragma unroll
+              for (int j = 0; j < 32; ++j)
+                if (n + 32 + j < P)
+                  pool[n + 32 + j] = make_key(Tr::kFolded ? db[j] : db[j] + qn, (uint32_t)(col0 + 32 + j));
+              n += 64;
+              ma = mb = 0u;
+              STAT_INC(st_surv, 64);
+            }
             auto take = [&](uint32_t& m, const float (&dv)[32], int c0) {
               if (m) {
                 const int j = __ffs(m) - 1;
@@ -714,6 +743,9 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
             }
           }
         }
+        if (p.minima && valid)
+          p.minima[(size_t)q * (2 * (size_t)p.num_tiles) + 2 * (size_t)tphys + g] =
+              Tr::kFolded ? bmin : bmin + qn;
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(&acc_empty[slot]);
@@ -744,7 +776,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
       if (!ok) break;
       // a refresh may keep a few more than k' keys (unsorted): record them all;
       // the merge pass selects exactly
-      if (valid && g == 0) {
+      if (valid && g == 0 && !p.minima) {
         const int cn = cnt_s[row];
         p.pool_counts[(pool_row0 + row) * U + u_ord] = cn < P ? cn : P;
         if (gap) p.pool_counts[(pool_row0 + row) * U + u_ord - 1] = 0;
@@ -796,14 +828,14 @@ EncodeTiledFn get_encode_fn() {
 
 // 2-D K-major operand map: rows x ld elements, box = (128 bytes of K) x box_rows
 // with the 128-byte swizzle, or (narrow) 32 bytes of K with the 32-byte
-// swizzle; zero fill out of bounds.
+// swizzle; zero fill out of bounds.  Map row j is stored row j * row_step.
 bool make_map(CUtensorMap* m, const void* base, bool fp8, long long rows, long long ld_elems, int box_rows,
-              bool narrow = false) {
+              bool narrow = false, int row_step = 1) {
   EncodeTiledFn fn = get_encode_fn();
   if (!fn) return false;
   const int esz = fp8 ? 1 : 2;
   cuuint64_t dims[2] = {(cuuint64_t)ld_elems, (cuuint64_t)rows};
-  cuuint64_t strides[1] = {(cuuint64_t)(ld_elems * esz)};
+  cuuint64_t strides[1] = {(cuuint64_t)(ld_elems * esz * (row_step > 1 ? row_step : 1))};
   cuuint32_t box[2] = {(cuuint32_t)((narrow ? kTailRowBytes : kChunkBytes) / esz), (cuuint32_t)box_rows};
   cuuint32_t estr[2] = {1, 1};
   CUresult r = fn(m, fp8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
@@ -864,16 +896,19 @@ cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, 
     it.pools = f.pools;
     it.pool_counts = f.pool_counts;
     it.q_bound = f.q_bound;
-    it.q_bound_half = f.q_bound_half;
+    it.db_step = f.db_step > 1 ? f.db_step : 1;
+    it.minima = f.minima;
     CUtensorMap* m = &a.maps[i * kMapsPerItem];
     const void* qh = fp8 ? (const void*)f.q8 : (const void*)f.qh;
     const void* xh = fp8 ? (const void*)f.x8 : (const void*)f.xh;
     const long long ldq = fp8 ? f.ld8 : f.ld16;
-    if (!make_map(&m[kMapQHi], qh, fp8, f.nq_pad, ldq, kBM) || !make_map(&m[kMapXHi], xh, fp8, f.nb_pad, ldq, kBN))
+    const int step = it.db_step;
+    if (!make_map(&m[kMapQHi], qh, fp8, f.nq_pad, ldq, kBM) ||
+        !make_map(&m[kMapXHi], xh, fp8, f.nb_pad, ldq, kBN, false, step))
       return cudaErrorInvalidValue;
     if (FORM == kFormExact) {
       if (!make_map(&m[kMapQLo], f.ql, false, f.nq_pad, f.ld16, kBM) ||
-          !make_map(&m[kMapXLo], f.xl, false, f.nb_pad, f.ld16, kBN))
+          !make_map(&m[kMapXLo], f.xl, false, f.nb_pad, f.ld16, kBN, false, step))
         return cudaErrorInvalidValue;
     } else {
       m[kMapQLo] = m[kMapQHi];
@@ -881,7 +916,7 @@ cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, 
     }
     if (FORM != kFormFP8) {
       if (!make_map(&m[kMapQTail], f.qh, false, f.nq_pad, f.ld16, kBM, true) ||
-          !make_map(&m[kMapXTail], f.xh, false, f.nb_pad, f.ld16, kBN, true))
+          !make_map(&m[kMapXTail], f.xh, false, f.nb_pad, f.ld16, kBN, true, step))
         return cudaErrorInvalidValue;
     } else {
       m[kMapQTail] = m[kMapQHi];
@@ -1014,7 +1049,8 @@ cudaError_t launch_fused(const FusedLaunch& f, cudaStream_t st) {
   s.pools = f.pools;
   s.pool_counts = f.pool_counts;
   s.q_bound = f.q_bound;
-  s.q_bound_half = f.q_bound_half;
+  s.db_step = f.db_step;
+  s.minima = f.minima;
   FusedItemPlan ip;
   ip.num_qblocks = f.plan.num_qblocks;
   ip.num_tiles = f.plan.num_tiles;

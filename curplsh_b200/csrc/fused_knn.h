@@ -53,11 +53,14 @@ struct FusedLaunch {
   const uint8_t* x8;
   const float* xn;
   const float* xs;
+  // database row j of this pass is stored row j * db_step (a strided sample when > 1)
+  int db_step = 1;
+  // non-null: block-minimum mode, see FusedItem::minima (pools are not used)
+  float* minima = nullptr;
   // outputs / scratch
   uint64_t* pools;
   int* pool_counts;
   uint32_t* q_bound;
-  uint32_t* q_bound_half;  // [nq_pad][2]
   uint32_t* status;
   unsigned long long* stats = nullptr;  // instrumented builds only
   FusedPlan plan;
@@ -90,10 +93,11 @@ struct FusedItemSpec {
   const uint8_t* x8;
   const float* xn;
   const float* xs;
-  uint64_t* pools;          // [G*128][U][2][pool_cap]
-  int* pool_counts;         // [G*128][U][2]
-  uint32_t* q_bound;        // [nq_pad], initialised to all ones
-  uint32_t* q_bound_half;   // [nq_pad][2], initialised to all ones
+  uint64_t* pools;          // [G*128][U][pool_cap]
+  int* pool_counts;         // [G*128][U]
+  uint32_t* q_bound;        // [nq_pad], initialised to all ones (or to estimated bounds)
+  int db_step;              // database row j is stored row j * db_step (0 or 1: contiguous)
+  float* minima;            // non-null: block-minimum mode (FusedItem::minima)
 };
 struct FusedItemPlan {
   int num_qblocks, num_tiles, units_per_block;
@@ -156,7 +160,8 @@ struct MergeLaunch {
   const uint64_t* pools;
   const int* pool_counts;
   const uint32_t* q_bound;       // final bounds of the fused pass (may be null)
-  const uint32_t* q_bound_half;  // [nq_pad][2]
+  int* fail_count = nullptr;     // see MergeItem
+  int* fail_list = nullptr;
   const float* queries;   // [nq x d] fp32, row stride d
   const float* db;        // [nb x d] fp32, row stride ld_db
   long long ld_db;
@@ -183,7 +188,11 @@ struct MergeItem {
   const uint64_t* pools;   // the fused item's pools and counts
   const int* pool_counts;
   const uint32_t* q_bound;       // the fused item's final bounds by pool row (may be null)
-  const uint32_t* q_bound_half;  // [rows][2]
+  // Non-null when the fused pass started from estimated bounds: a query with
+  // fewer than k' candidates under its final bound may miss rows, so its
+  // index within the item is appended to fail_list (count in *fail_count).
+  int* fail_count;
+  int* fail_list;
   const float* queries;    // [nq x d] fp32, row stride d
   const float* db;         // database rows fp32, row stride ld_db
   long long ld_db;
@@ -197,6 +206,14 @@ cudaError_t prepare_merge_kernel();
 
 // Fill [n] ints / floats (N == 0 results, padding).
 cudaError_t launch_fill_results(int* idx, float* dist, long long n, cudaStream_t st);
+// out[q] = order bits of the j-th smallest (1-based) of minima[q * count ..
+// q * count + count) for q < nq (all ones when count < j).
+cudaError_t launch_estimate_select(const float* minima, int count, int nq, int j, uint32_t* out, cudaStream_t st);
+// dst[i] = src[rows[i]] for i < n (rows of d floats).
+cudaError_t launch_gather_rows(const float* src, int d, const int* rows, int n, float* dst, cudaStream_t st);
+// out[rows[i]] = in[i] for i < n (result rows of k indices and distances).
+cudaError_t launch_scatter_results(const int* in_idx, const float* in_dist, const int* rows, int n, int k,
+                                   int* out_idx, float* out_dist, cudaStream_t st);
 
 }  // namespace curplsh_b200
 

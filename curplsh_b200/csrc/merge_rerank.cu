@@ -123,13 +123,10 @@ __global__ void __launch_bounds__(kMergeThreads) merge_rerank_kernel(const __gri
   const int nlists = T > 0 ? (int)(last - first + 1 + (T - 1) / m.split_tiles) : 0;
   const size_t list0 = ((size_t)qb * kBM + row) * U;  // pool-list index of unit 0
   // Final bound of the fused pass on this query's k'-th coarse distance: the
-  // smallest k'-th of any pool, and the larger of the per-half (k'/2)-th
-  // bounds.  Every key of the k' smallest has a distance <= it.
+  // smallest k'-th of any pool, or the estimate the pass started from.  When
+  // it comes from a pool, every key of the k' smallest has a distance <= it.
   uint32_t qbound = 0xFFFFFFFFu;
-  if (m.q_bound && T > 0 && a.pre_cap > 0) {
-    const uint32_t h0 = m.q_bound_half[2 * (size_t)prow], h1 = m.q_bound_half[2 * (size_t)prow + 1];
-    qbound = min(m.q_bound[prow], max(h0, h1));
-  }
+  if (m.q_bound && T > 0 && a.pre_cap > 0) qbound = m.q_bound[prow];
 
   for (int i = tid; i < d; i += kMergeThreads) qv[i] = m.queries[(size_t)q * d + i];
   if (tid == 0) {
@@ -162,16 +159,29 @@ __global__ void __launch_bounds__(kMergeThreads) merge_rerank_kernel(const __gri
   } else {
     for (int l = 0; l < nlists; ++l) cnt += lcnt[l];
   }
+  // Started from an estimate E: every row with a key under E was admitted, so
+  // k' keys under the final bound (<= E) prove that the k' smallest keys of
+  // the whole database are among the candidates (their k'-th is then <= E, and
+  // a pool selection never drops one of them).  Fewer: E may have been too
+  // small, and the query is listed for a search without the estimate.
+  if (m.fail_count && cnt < m.kprime && tid == 0) {
+    const int pos = atomicAdd(m.fail_count, 1);
+    m.fail_list[pos] = q;
+  }
   const int keep = cnt < m.kprime ? cnt : m.kprime;
   // ---- 2. select the k' smallest (in shared memory unless too many passed)
   uint64_t bound = ~0ull;
-  if (cnt <= a.pre_cap) {
-    if (cnt > keep)
+  if (cnt > keep) {
+    if (cnt <= a.pre_cap)
       bound = block_select_bound(
           [&](auto f) {
             for (int i = tid; i < cnt; i += kMergeThreads) f(pre[i]);
           },
           (uint32_t)keep, hist, warp_tot, misc);
+    else
+      bound = block_select_bound(each_pool_key, (uint32_t)keep, hist, warp_tot, misc);
+  }
+  if (cnt <= a.pre_cap) {
     for (int i = tid; i < cnt; i += kMergeThreads) {
       const uint64_t key = pre[i];
       if (key <= bound) {
@@ -180,7 +190,6 @@ __global__ void __launch_bounds__(kMergeThreads) merge_rerank_kernel(const __gri
       }
     }
   } else {
-    if (cnt > keep) bound = block_select_bound(each_pool_key, (uint32_t)keep, hist, warp_tot, misc);
     each_pool_key([&](uint64_t key) {
       if (key <= bound) {
         const uint32_t pos = atomicAdd(&misc[4], 1u);
@@ -347,6 +356,8 @@ cudaError_t launch_merge_batch(MergeItem* items, int n, int d, uint32_t* status,
     long long len = std::min<long long>(items[i].split_tiles, items[i].work_per_cta);
     len = std::min<long long>(len, items[i].num_tiles);
     bounded = bounded || (items[i].q_bound && len * kBN >= items[i].kprime);
+    // the estimate check counts the keys under the final bound
+    bounded = bounded || (items[i].q_bound && items[i].fail_count);
   }
   a.pre_cap = bounded ? 2 * kp2 : 0;
   a.lcnt_n = (umax + 3) & ~3;
@@ -379,7 +390,8 @@ cudaError_t launch_merge_rerank(const MergeLaunch& m, cudaStream_t st) {
   it.pools = m.pools;
   it.pool_counts = m.pool_counts;
   it.q_bound = m.q_bound;
-  it.q_bound_half = m.q_bound_half;
+  it.fail_count = m.fail_count;
+  it.fail_list = m.fail_list;
   it.queries = m.queries;
   it.db = m.db;
   it.ld_db = m.ld_db;

@@ -154,13 +154,13 @@ int MultiPlan::build(const curplsh_batch_item* items, int n, const std::vector<c
   };
   o_status_ = take(sizeof(uint32_t));
   bounds_words_ = 0;
-  for (const FItem& x : fitems_) bounds_words_ += 3 * (size_t)x.nq_pad;
+  for (const FItem& x : fitems_) bounds_words_ += (size_t)x.nq_pad;
   o_bounds_ = take(bounds_words_ * sizeof(uint32_t));
   size_t bcur = 0;
   for (FItem& x : fitems_) {
     const IndexView& v = views[x.slot];
     x.o_bounds = o_bounds_ + bcur * sizeof(uint32_t);
-    bcur += 3 * (size_t)x.nq_pad;
+    bcur += (size_t)x.nq_pad;
     if (v.n == 0) continue;
     const size_t lists = (size_t)x.plan.num_qblocks * kBM * x.plan.units_per_block;
     if (x.form != kFormFP8) x.o_qh = take((size_t)x.nq_pad * v.ld16 * 2);
@@ -194,7 +194,6 @@ void MultiPlan::bind(void* base_v) {
     s.ld16 = v.ld16;
     s.ld8 = v.ld8;
     s.q_bound = reinterpret_cast<uint32_t*>(base + x.o_bounds);
-    s.q_bound_half = s.q_bound + x.nq_pad;
     if (v.n == 0) continue;
     s.qh = x.o_qh ? reinterpret_cast<__nv_bfloat16*>(base + x.o_qh) : nullptr;
     s.ql = x.o_ql ? reinterpret_cast<__nv_bfloat16*>(base + x.o_ql) : nullptr;
@@ -302,7 +301,8 @@ int MultiPlan::enqueue(cudaStream_t main, const std::vector<cudaStream_t>* branc
         m.pools = x.spec.pools;
         m.pool_counts = x.spec.pool_counts;
         m.q_bound = x.spec.q_bound;
-        m.q_bound_half = x.spec.q_bound_half;
+        m.fail_count = nullptr;
+        m.fail_list = nullptr;
         m.queries = it.queries;
         m.db = v.x32;
         m.ld_db = v.dim;

@@ -97,7 +97,7 @@ Layout carve(int form, long long nq_pad, long long ld16, long long ld8, size_t p
   L.q8 = form == kFormFP8 ? take((size_t)nq_pad * ld8) : 0;
   L.qn = take((size_t)nq_pad * 4);
   L.qs = take((size_t)nq_pad * 4);
-  L.qbound = take((size_t)nq_pad * 12);  // k'-th bounds, then two half bounds per query
+  L.qbound = take((size_t)nq_pad * 4);  // k'-th bounds
   L.counts = take(pool_lists * 4);
   L.pools = take(pool_lists * (size_t)P * 8);
   L.total = off;
@@ -179,7 +179,7 @@ int search_noalloc_locked(const IndexView& v, int nq, const float* q, int k, int
 
   // state that must start cleared on every call (the array keeps the last call's contents)
   NA_TRY(cudaMemsetAsync(status, 0, sizeof(uint32_t), st));
-  NA_TRY(cudaMemsetAsync(qbound, 0xFF, (size_t)3 * nq_pad * sizeof(uint32_t), st));
+  NA_TRY(cudaMemsetAsync(qbound, 0xFF, (size_t)nq_pad * sizeof(uint32_t), st));
   NA_TRY(launch_prep_rows(q, v.dim, nq, nq_pad, v.dim, qn, 0.f, form == kFormFP8 ? nullptr : qh, ql, v.ld16, q8,
                           qs, v.ld8, st, form == kFormFP8 ? kAugNone : kAugQuery));
   FusedLaunch f{};
@@ -206,7 +206,6 @@ int search_noalloc_locked(const IndexView& v, int nq, const float* q, int k, int
   f.pools = pools;
   f.pool_counts = counts;
   f.q_bound = qbound;
-  f.q_bound_half = qbound + nq_pad;
   f.status = status;
   f.plan = plan;
   NA_TRY(launch_fused(f, st));
@@ -221,7 +220,6 @@ int search_noalloc_locked(const IndexView& v, int nq, const float* q, int k, int
   m.pools = pools;
   m.pool_counts = counts;
   m.q_bound = qbound;
-  m.q_bound_half = qbound + nq_pad;
   m.queries = q;
   m.db = v.x32;
   m.ld_db = v.dim;

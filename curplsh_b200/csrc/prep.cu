@@ -240,6 +240,91 @@ __global__ void fill_results_kernel(int* idx, float* dist, long long n) {
   }
 }
 
+// One warp per query: the j-th smallest (1-based) of `count` floats, by a
+// most-significant-digit radix select on their order bits (4 passes of 8
+// bits, a 256-bin warp histogram in shared memory).
+constexpr int kSelectWarps = 8;
+__global__ void __launch_bounds__(kSelectWarps * 32)
+    estimate_select_kernel(const float* __restrict__ minima, int count, int nq, int j, uint32_t* __restrict__ out) {
+  __shared__ uint32_t hist_all[kSelectWarps][256];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int q = blockIdx.x * kSelectWarps + warp;
+  if (q >= nq) return;
+  if (count < j || j < 1) {
+    if (lane == 0) out[q] = kOrdInf;
+    return;
+  }
+  uint32_t* hist = hist_all[warp];
+  const float* v = minima + (size_t)q * count;
+  uint32_t prefix = 0, mask = 0, rank = (uint32_t)j;
+  for (int shift = 24; shift >= 0; shift -= 8) {
+#pragma unroll
+    for (int b = 0; b < 8; ++b) hist[lane * 8 + b] = 0u;
+    __syncwarp();
+    for (int i = lane; i < count; i += 32) {
+      const uint32_t o = f2ord(v[i]);
+      if ((o & mask) == prefix) atomicAdd(&hist[(o >> shift) & 255u], 1u);
+    }
+    __syncwarp();
+    // the digit whose bucket holds the rank-th key: lane l sums bins 8l..8l+7
+    uint32_t c[8], s = 0;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      c[b] = hist[lane * 8 + b];
+      s += c[b];
+    }
+    uint32_t incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const uint32_t excl = incl - s;
+    const bool mine = excl < rank && rank <= incl;
+    uint32_t digit = 0, before = 0;
+    if (mine) {
+      uint32_t acc = excl;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        if (acc < rank && rank <= acc + c[b]) {
+          digit = (uint32_t)(lane * 8 + b);
+          before = acc;
+        }
+        acc += c[b];
+      }
+    }
+    const int src = __ffs(__ballot_sync(0xffffffffu, mine)) - 1;
+    digit = __shfl_sync(0xffffffffu, digit, src);
+    before = __shfl_sync(0xffffffffu, before, src);
+    prefix |= digit << shift;
+    mask |= 255u << shift;
+    rank -= before;
+    __syncwarp();
+  }
+  if (lane == 0) out[q] = prefix;
+}
+
+// One block per listed row: dst row i <- src row rows[i].
+__global__ void gather_rows_kernel(const float* __restrict__ src, int d, const int* __restrict__ rows,
+                                   float* __restrict__ dst) {
+  const int i = blockIdx.x;
+  const float* s = src + (size_t)rows[i] * d;
+  float* t = dst + (size_t)i * d;
+  for (int c = threadIdx.x; c < d; c += blockDim.x) t[c] = s[c];
+}
+
+// One block per listed row: result row rows[i] <- row i.
+__global__ void scatter_results_kernel(const int* __restrict__ in_idx, const float* __restrict__ in_dist,
+                                       const int* __restrict__ rows, int k, int* __restrict__ out_idx,
+                                       float* __restrict__ out_dist) {
+  const int i = blockIdx.x;
+  const size_t o = (size_t)rows[i] * k, s = (size_t)i * k;
+  for (int c = threadIdx.x; c < k; c += blockDim.x) {
+    out_idx[o + c] = in_idx[s + c];
+    out_dist[o + c] = in_dist[s + c];
+  }
+}
+
 }  // namespace
 
 cudaError_t launch_prep_rows(const float* x, long long ldx, int nrows, long long nrows_pad, int d, float* norms,
@@ -290,6 +375,26 @@ cudaError_t launch_fill_results(int* idx, float* dist, long long n, cudaStream_t
   long long blocks = (n + 255) / 256;
   if (blocks > 4096) blocks = 4096;
   fill_results_kernel<<<(unsigned)blocks, 256, 0, st>>>(idx, dist, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_rows(const float* src, int d, const int* rows, int n, float* dst, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  gather_rows_kernel<<<(unsigned)n, 128, 0, st>>>(src, d, rows, dst);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_results(const int* in_idx, const float* in_dist, const int* rows, int n, int k,
+                                   int* out_idx, float* out_dist, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  scatter_results_kernel<<<(unsigned)n, 128, 0, st>>>(in_idx, in_dist, rows, k, out_idx, out_dist);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_estimate_select(const float* minima, int count, int nq, int j, uint32_t* out, cudaStream_t st) {
+  if (nq <= 0) return cudaSuccess;
+  estimate_select_kernel<<<(unsigned)((nq + kSelectWarps - 1) / kSelectWarps), kSelectWarps * 32, 0, st>>>(
+      minima, count, nq, j, out);
   return cudaGetLastError();
 }
 

@@ -121,8 +121,10 @@ int curplsh_index_search(curplsh_index* index, int64_t num, const float* queries
 int curplsh_index_search_ex(curplsh_index* index, int64_t num, const float* queries, int k, int precision,
                             int rerank_factor, int* indices, float* distances, void* stream);
 /* As curplsh_index_search_ex, synchronous, also returning device-timed milliseconds of the passes
- * (CUDA events on the launching stream): pass_ms[0] query prep, [1] fused tensor-core filter,
- * [2] merge + exact rerank, [3] whole search including any host<->device copies. */
+ * (CUDA events on the launching stream): pass_ms[0] query prep (and the sampled bound estimate when
+ * one is used), [1] fused tensor-core filter over the whole database, [2] merge + exact rerank,
+ * [3] whole search including any host<->device copies and any re-search of queries whose
+ * estimate failed. */
 int curplsh_index_search_profiled(curplsh_index* index, int64_t num, const float* queries, int k,
                                   int precision, int rerank_factor, int* indices, float* distances,
                                   void* stream, float* pass_ms);
@@ -271,6 +273,26 @@ int curplsh_tuning_set(int precision, int dim, int k, int64_t num_queries, int s
 /* Writes the bucket's parameters (the defaults when it was never set). */
 int curplsh_tuning_get(int precision, int dim, int k, int64_t num_queries, int* split_q4, int* pool_headroom);
 int curplsh_tuning_clear(void);
+
+/* ------------------------------------------------------------ sampled bound estimate */
+/* No counterpart in the reference.  A search of many queries against a large database
+ * (curplsh_index_search / _ex / _profiled) may first run the fused pass over a strided sample of
+ * the database, keeping per query the smallest distance of every 128-row block of the sample,
+ * and start every candidate pool of the full pass at the j-th smallest of those block minima,
+ * so far fewer rows survive the filter.  The merge pass verifies the estimate exactly (k'
+ * candidates under the final bound prove the result complete); queries it fails are searched
+ * again without it before the call returns, so results are identical with the estimate on or
+ * off.  A search that uses it returns synchronised even with device buffers.  The switch is
+ * process-wide; on (1) by default. */
+int curplsh_set_bound_estimate(int enabled);
+int curplsh_get_bound_estimate(int* enabled);
+/* The estimate a search of num_queries queries with this k / precision / rerank factor would
+ * use: *sample_rows = 0 when none, else the sample size, its row step and the rank j among the
+ * sample_rows / 128 block minima. */
+int curplsh_index_estimate_plan(curplsh_index* index, int64_t num_queries, int k, int precision,
+                                int rerank_factor, int* sample_rows, int* step, int* rank);
+/* Number of queries this index searched again after their estimate failed (since creation). */
+int curplsh_index_get_fallback_count(curplsh_index* index, int64_t* count);
 
 #ifdef __cplusplus
 } /* extern "C" */
