@@ -343,7 +343,11 @@ double binomial_tail(int n, double q, int j) {
   return t;
 }
 
-constexpr double kEstimateMu = 12.0;        // expected sample rows among a query's k' nearest
+// mu = expected sample rows among a query's k' nearest.  A larger sample gives
+// a tighter rank (j / mu falls from ~2.6 at mu = 12 to ~2 at 24) but costs
+// more; the sample pass takes at most a tenth of the full pass's tiles.
+constexpr double kEstimateMuMax = 24.0;
+constexpr double kEstimateMuMin = 8.0;
 constexpr double kEstimateFailure = 1e-6;   // per-query failure probability for a uniform sample
 constexpr int kEstimateBlockRows = kHalfN;  // rows per block minimum (one epilogue warp's half tile)
 
@@ -352,8 +356,9 @@ EstimatePlan plan_estimate(int nq, long long n, int kp, int num_sms) {
   if (!g_bound_estimate.load(std::memory_order_relaxed) || nq < 1 || kp < 1) return e;
   if (n < (1LL << 16) || n < 64LL * kp) return e;  // a short search gains too little
   const long long T = (n + kBN - 1) / kBN;
-  const long long tiles = (long long)std::ceil(kEstimateMu * (double)n / kp / kBN);
-  if (tiles * 10 > T) return e;  // the sample pass must cost at most a tenth of the full pass
+  long long tiles = (long long)std::ceil(kEstimateMuMax * (double)n / kp / kBN);
+  tiles = std::min(tiles, T / 10);
+  if ((double)kp * tiles * kBN / (double)n < kEstimateMuMin) return e;  // too small a sample
   e.rows = (int)(tiles * kBN);
   e.step = (int)(n / e.rows);  // >= 10; rows j * step < n for every j < rows
   e.blocks = e.rows / kEstimateBlockRows;

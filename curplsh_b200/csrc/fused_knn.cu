@@ -648,13 +648,20 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
             // block-minimum mode: no survivors, only the half tile's smallest
             // distance (columns past nb excluded)
             const int lim = p.nb - col0;
-            float m0 = 3.402823466e38f, m1 = 3.402823466e38f;
+            float mm[16];
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
-              if (j < lim) m0 = fminf(m0, da[j]);
-              if (32 + j < lim) m1 = fminf(m1, db[j]);
+            for (int j = 0; j < 16; ++j) {  // a tree, not one dependent chain
+              const float a0 = j < lim ? da[j] : 3.402823466e38f;
+              const float a1 = 16 + j < lim ? da[16 + j] : 3.402823466e38f;
+              const float b0 = 32 + j < lim ? db[j] : 3.402823466e38f;
+              const float b1 = 48 + j < lim ? db[16 + j] : 3.402823466e38f;
+              mm[j] = fminf(fminf(a0, a1), fminf(b0, b1));
             }
-            bmin = fminf(bmin, fminf(m0, m1));
+#pragma unroll
+            for (int w = 8; w > 0; w >>= 1)
+#pragma unroll
+              for (int j = 0; j < w; ++j) mm[j] = fminf(mm[j], mm[j + w]);
+            bmin = fminf(bmin, mm[0]);
             continue;
           }
           // survivor masks, each OR-combined in four independent partial masks
