@@ -273,7 +273,10 @@ __device__ __forceinline__ float select32(const float (&v)[32], int j) {
 }
 
 // ------------------------------------------------------------------ kernel
-template <int FORM, int MAXI>
+// MINIMA selects the block-minimum mode (FusedItem::minima, the sample pass of
+// the bound estimate) at compile time, so the candidate-pool kernel carries
+// none of its code.
+template <int FORM, int MAXI, bool MINIMA = false>
 __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_constant__ FusedArgs<MAXI> A) {
   using Tr = FormTraits<FORM>;
   const FusedBatch& B = A.B;
@@ -585,7 +588,8 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
             // < nb_pad: rows are padded to whole tiles (a strided sample has no padding)
-            const size_t c = (size_t)(tphys * kBN + g * kHalfN + lane + 32 * i) * (size_t)p.db_step;
+            const int c0 = tphys * kBN + g * kHalfN + lane + 32 * i;
+            const size_t c = MINIMA ? (size_t)c0 * (size_t)p.db_step : (size_t)c0;
             pxn[i] = __ldg(p.db_norms + c);
             psx[i] = __ldg(p.db_scale + c);
           }
@@ -644,7 +648,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
               fma2_f32(dst[o + 2], dst[o + 3], p2, p3, m2s, m2s, xn.z, xn.w);
             }
           }
-          if (p.minima) {
+          if (MINIMA) {
             // block-minimum mode: no survivors, only the half tile's smallest
             // distance (columns past nb excluded)
             const int lim = p.nb - col0;
@@ -750,7 +754,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
             }
           }
         }
-        if (p.minima && valid)
+        if (MINIMA && valid)
           p.minima[(size_t)q * (2 * (size_t)p.num_tiles) + 2 * (size_t)tphys + g] =
               Tr::kFolded ? bmin : bmin + qn;
         tc_fence_before();
@@ -783,7 +787,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
       if (!ok) break;
       // a refresh may keep a few more than k' keys (unsorted): record them all;
       // the merge pass selects exactly
-      if (valid && g == 0 && !p.minima) {
+      if (!MINIMA && valid && g == 0) {
         const int cn = cnt_s[row];
         p.pool_counts[(pool_row0 + row) * U + u_ord] = cn < P ? cn : P;
         if (gap) p.pool_counts[(pool_row0 + row) * U + u_ord - 1] = 0;
@@ -853,13 +857,13 @@ bool make_map(CUtensorMap* m, const void* base, bool fp8, long long rows, long l
 }
 
 // Raises the kernel's dynamic shared memory limit once per device.
-template <int FORM, int MAXI>
+template <int FORM, int MAXI, bool MINIMA = false>
 cudaError_t ensure_attributes() {
   static bool attr_done[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr_done[dev & 63]) {
-    cudaError_t e = cudaFuncSetAttribute(fused_knn_kernel<FORM, MAXI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(fused_knn_kernel<FORM, MAXI, MINIMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          227 * 1024);
     if (e != cudaSuccess) return e;
     attr_done[dev & 63] = true;
@@ -867,10 +871,10 @@ cudaError_t ensure_attributes() {
   return cudaSuccess;
 }
 
-template <int FORM, int MAXI>
+template <int FORM, int MAXI, bool MINIMA = false>
 cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, int n, const FusedBatchPlan& bp,
                         uint32_t* status, unsigned long long* stats, uint32_t smem, cudaStream_t st) {
-  cudaError_t e = ensure_attributes<FORM, MAXI>();
+  cudaError_t e = ensure_attributes<FORM, MAXI, MINIMA>();
   if (e != cudaSuccess) return e;
   FusedArgs<MAXI> a;
   memset(&a, 0, sizeof(a));
@@ -930,13 +934,16 @@ cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, 
       m[kMapXTail] = m[kMapXHi];
     }
   }
-  fused_knn_kernel<FORM, MAXI><<<bp.grid, kNumThreads, smem, st>>>(a);
+  fused_knn_kernel<FORM, MAXI, MINIMA><<<bp.grid, kNumThreads, smem, st>>>(a);
   return cudaGetLastError();
 }
 
 template <int FORM>
 cudaError_t launch_form_any(const FusedItemSpec* specs, const FusedItemPlan* plans, int n, const FusedBatchPlan& bp,
                             uint32_t* status, unsigned long long* stats, uint32_t smem, cudaStream_t st) {
+  if (n == 1 && specs[0].minima) return launch_form<FORM, 1, true>(specs, plans, n, bp, status, stats, smem, st);
+  for (int i = 0; i < n; ++i)
+    if (specs[i].minima) return cudaErrorInvalidValue;  // block-minimum mode is single-item
   if (n == 1) return launch_form<FORM, 1>(specs, plans, n, bp, status, stats, smem, st);
   return launch_form<FORM, kFusedMaxItems>(specs, plans, n, bp, status, stats, smem, st);
 }
