@@ -668,17 +668,31 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
             bmin = fminf(bmin, mm[0]);
             continue;
           }
-          // survivor masks, each OR-combined in four independent partial masks
-          uint32_t ma, mb;
-          {
-            uint32_t pa[4] = {0u, 0u, 0u, 0u}, pb[4] = {0u, 0u, 0u, 0u};
+          // The exact form's bound admits few rows: a tree minimum of the 64
+          // distances first, masks only when some lane's minimum passes (measured
+          // slower for the coarse forms, whose chunks pass more often).
+          bool any_pass = true;
+          if (FORM == kFormExact) {
+            float mm[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) mm[j] = fminf(fminf(da[j], da[16 + j]), fminf(db[j], db[16 + j]));
+#pragma unroll
+            for (int w = 8; w > 0; w >>= 1)
+#pragma unroll
+              for (int j = 0; j < w; ++j) mm[j] = fminf(mm[j], mm[j + w]);
+            any_pass = __any_sync(0xffffffffu, mm[0] <= thr);
+          }
+          // survivor masks, each OR-combined in eight independent partial masks
+          uint32_t ma = 0u, mb = 0u;
+          if (any_pass) {
+            uint32_t pa[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u}, pb[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
-              pa[j & 3] |= (da[j] <= thr ? 1u : 0u) << j;
-              pb[j & 3] |= (db[j] <= thr ? 1u : 0u) << j;
+              pa[j & 7] |= (da[j] <= thr ? 1u : 0u) << j;
+              pb[j & 7] |= (db[j] <= thr ? 1u : 0u) << j;
             }
-            ma = (pa[0] | pa[1]) | (pa[2] | pa[3]);
-            mb = (pb[0] | pb[1]) | (pb[2] | pb[3]);
+            ma = ((pa[0] | pa[1]) | (pa[2] | pa[3])) | ((pa[4] | pa[5]) | (pa[6] | pa[7]));
+            mb = ((pb[0] | pb[1]) | (pb[2] | pb[3])) | ((pb[4] | pb[5]) | (pb[6] | pb[7]));
           }
           if (!valid) ma = mb = 0u;
           // database rows beyond nb (padding of the last tile) never survive
