@@ -668,23 +668,9 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
             bmin = fminf(bmin, mm[0]);
             continue;
           }
-          // The exact form's bound admits few rows: a tree minimum of the 64
-          // distances first, masks only when some lane's minimum passes (measured
-          // slower for the coarse forms, whose chunks pass more often).
-          bool any_pass = true;
-          if (FORM == kFormExact) {
-            float mm[16];
-#pragma unroll
-            for (int j = 0; j < 16; ++j) mm[j] = fminf(fminf(da[j], da[16 + j]), fminf(db[j], db[16 + j]));
-#pragma unroll
-            for (int w = 8; w > 0; w >>= 1)
-#pragma unroll
-              for (int j = 0; j < w; ++j) mm[j] = fminf(mm[j], mm[j + w]);
-            any_pass = __any_sync(0xffffffffu, mm[0] <= thr);
-          }
           // survivor masks, each OR-combined in eight independent partial masks
           uint32_t ma = 0u, mb = 0u;
-          if (any_pass) {
+          {
             uint32_t pa[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u}, pb[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
