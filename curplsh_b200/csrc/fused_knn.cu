@@ -558,8 +558,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
           const int r = lg * 32 + src;
           const int n_src = cnt_s[r];
           int kept = 0;
-          uint64_t half_key = 0;
-          const uint64_t kmax = warp_select_keep_any(pool_of(r), n_src < P ? n_src : P, keep, P, hist, kept, half_key);
+          const uint64_t kmax = warp_select_keep_any(pool_of(r), n_src < P ? n_src : P, keep, P, hist, kept);
           if (lane == src) {
             const uint32_t ord = (uint32_t)(kmax >> 32);
             cnt_s[r] = kept;

@@ -82,12 +82,11 @@ __device__ __forceinline__ uint64_t warp_max_u64(uint64_t v) {
 // starting at the highest bit in which the considered keys differ, so bits
 // they all share cost no pass.  `hist` is a 256-entry warp-private shared
 // buffer.  Returns a key bound B such that exactly `rank` of the considered
-// keys are <= B; `half_bound` gets a key with at least `half_rank` considered
-// keys <= it (the upper edge of the first pass's bin that holds that rank).
-// Requires 1 <= half_rank <= rank <= number of considered keys.  Warp-collective.
+// keys are <= B.  Requires 1 <= rank <= number of considered keys.
+// Warp-collective.
 template <int E>
 __device__ __forceinline__ uint64_t warp_radix_bound(const uint64_t (&key)[E], uint64_t limit, uint32_t rank,
-                                                     uint32_t half_rank, uint32_t* hist, uint64_t& half_bound) {
+                                                     uint32_t* hist) {
   const int lane = threadIdx.x & 31;
   uint64_t lo = ~0ull, hi = 0;
 #pragma unroll
@@ -104,8 +103,6 @@ __device__ __forceinline__ uint64_t warp_radix_bound(const uint64_t (&key)[E], u
   // bits at and above shift+8 are common to every considered key
   uint64_t pmask = shift + 8 >= 64 ? 0ull : ~((1ull << (shift + 8)) - 1ull);
   uint64_t prefix = lo & pmask;
-  half_bound = ~0ull;
-  bool first = true;
   for (;;) {
 #pragma unroll
     for (int b = 0; b < 8; ++b) hist[lane * 8 + b] = 0u;
@@ -117,12 +114,6 @@ __device__ __forceinline__ uint64_t warp_radix_bound(const uint64_t (&key)[E], u
 #ifdef CURPLSH_FUSED_STATS
     if (lane == 0 && g_radix_pass_counter) atomicAdd(g_radix_pass_counter, 1ull);
 #endif
-    if (first) {
-      uint32_t hd, hb, hc;
-      radix_digit_step(hist, half_rank, hd, hb, hc);
-      half_bound = prefix | ((uint64_t)hd << shift) | ((1ull << shift) - 1ull);
-      first = false;
-    }
     uint32_t digit, before, cnt;
     radix_digit_step(hist, rank, digit, before, cnt);
     prefix |= (uint64_t)digit << shift;
@@ -148,39 +139,6 @@ __device__ __forceinline__ uint64_t warp_max_key_le(const uint64_t (&key)[E], ui
     m = v > m ? v : m;
   }
   return m;
-}
-
-// Keep exactly the `keep` smallest keys of pool[0..n) (requires n > keep >= 1),
-// compacted into pool[0..keep), for pools of at most 32*E entries held in
-// registers.  Returns (same in every lane) the largest kept key and the number
-// kept, and sets `half_key` to a key with at least ceil(keep/2) kept keys <= it.
-template <int E>
-__device__ __forceinline__ uint64_t warp_select_keep_reg(uint64_t* pool, int n, int keep, uint32_t* hist, int& kept,
-                                                         uint64_t& half_key) {
-  const int lane = threadIdx.x & 31;
-  uint64_t key[E];
-#pragma unroll
-  for (int e = 0; e < E; ++e) {
-    const int i = e * 32 + lane;
-    key[e] = i < n ? pool[i] : kKeyEmpty;
-  }
-  // empty slots hold the all-ones key, which `limit` excludes
-  uint64_t hb;
-  const uint64_t bound =
-      warp_radix_bound<E>(key, kKeyEmpty - 1, (uint32_t)keep, (uint32_t)((keep + 1) / 2), hist, hb);
-  int w = 0;
-#pragma unroll
-  for (int e = 0; e < E; ++e) {
-    const bool take = key[e] <= bound;
-    const uint32_t bal = __ballot_sync(0xffffffffu, take);
-    if (take) pool[w + __popc(bal & ((1u << lane) - 1u))] = key[e];
-    w += __popc(bal);
-  }
-  kept = w;
-  const uint64_t kmax = warp_max_key_le<E>(key, bound);
-  half_key = hb < kmax ? hb : kmax;
-  __syncwarp();
-  return kmax;
 }
 
 // Count of the warp's keys <= b (every lane gets the total).
@@ -227,12 +185,11 @@ __device__ __forceinline__ uint64_t warp_sample_find(const uint64_t (&key)[E], u
 // <= B where B is the smallest of 32 stratified sample keys with at least
 // `keep` keys <= B (so roughly keep + n/32 keys are kept).  B is a genuine
 // pool key, so the pool still holds at least `keep` keys <= its bound and the
-// bound stays a valid upper bound of the k'-th distance.  `half_key` gets the
-// smallest sample with at least ceil(keep/2) keys <= it.  Returns B; falls back
-// to the exact radix form when the samples cannot free enough room.
+// bound stays a valid upper bound of the k'-th distance.  Returns B; falls
+// back to the exact radix form when the samples cannot free enough room.
 template <int E>
 __device__ __forceinline__ uint64_t warp_select_keep_sampled(uint64_t* pool, int n, int keep, int cap,
-                                                             uint32_t* hist, int& kept, uint64_t& half_key) {
+                                                             uint32_t* hist, int& kept) {
   const int lane = threadIdx.x & 31;
   uint64_t key[E];
 #pragma unroll
@@ -257,14 +214,12 @@ __device__ __forceinline__ uint64_t warp_select_keep_sampled(uint64_t* pool, int
       smp = (lower == asc) ? mn : mx;
     }
   }
-  uint32_t c_keep = 0, c_half = 0;
+  uint32_t c_keep = 0;
   const uint64_t bound = warp_sample_find<E>(key, smp, n, (uint32_t)keep, c_keep);
   if (c_keep < (uint32_t)keep || bound == kKeyEmpty || (int)c_keep > cap - pool_sync_tiles(cap, keep) * kBN) {
     // samples too coarse to free a tile of room: exact selection
     __syncwarp();
-    uint64_t hb;
-    const uint64_t eb =
-        warp_radix_bound<E>(key, kKeyEmpty - 1, (uint32_t)keep, (uint32_t)((keep + 1) / 2), hist, hb);
+    const uint64_t eb = warp_radix_bound<E>(key, kKeyEmpty - 1, (uint32_t)keep, hist);
     int w = 0;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
@@ -275,11 +230,9 @@ __device__ __forceinline__ uint64_t warp_select_keep_sampled(uint64_t* pool, int
     }
     kept = w;
     const uint64_t kmax = warp_max_key_le<E>(key, eb);
-    half_key = hb < kmax ? hb : kmax;
     __syncwarp();
     return kmax;
   }
-  half_key = warp_sample_find<E>(key, smp, n, (uint32_t)((keep + 1) / 2), c_half);
   int w = 0;
 #pragma unroll
   for (int e = 0; e < E; ++e) {
@@ -333,12 +286,10 @@ __device__ __forceinline__ uint64_t warp_stream_max_le(const uint64_t* pool, int
 }
 
 __device__ __forceinline__ uint64_t warp_select_keep_stream(uint64_t* pool, int n, int keep, uint32_t* hist,
-                                                            int& kept, uint64_t& half_key) {
+                                                            int& kept) {
   const int lane = threadIdx.x & 31;
   const uint64_t bound = warp_stream_bound(pool, n, kKeyEmpty - 1, (uint32_t)keep, hist);
   const uint64_t kmax = warp_stream_max_le(pool, n, bound);
-  const uint64_t b2 = warp_stream_bound(pool, n, bound, (uint32_t)((keep + 1) / 2), hist);
-  half_key = warp_stream_max_le(pool, n, b2);  // large pools are rare: an exact second descent
   // in-place stable compaction: every read of a 32-entry round completes
   // (ballot) before any lane writes, and writes never pass the reads
   int w = 0;
@@ -357,10 +308,10 @@ __device__ __forceinline__ uint64_t warp_select_keep_stream(uint64_t* pool, int 
 
 // Dispatch on the pool capacity: registers up to 1024 entries, else streaming.
 __device__ __forceinline__ uint64_t warp_select_keep_any(uint64_t* pool, int n, int keep, int cap, uint32_t* hist,
-                                                         int& kept, uint64_t& half_key) {
-  if (cap <= 512) return warp_select_keep_sampled<16>(pool, n, keep, cap, hist, kept, half_key);
-  if (cap <= 1024) return warp_select_keep_sampled<32>(pool, n, keep, cap, hist, kept, half_key);
-  return warp_select_keep_stream(pool, n, keep, hist, kept, half_key);
+                                                         int& kept) {
+  if (cap <= 512) return warp_select_keep_sampled<16>(pool, n, keep, cap, hist, kept);
+  if (cap <= 1024) return warp_select_keep_sampled<32>(pool, n, keep, cap, hist, kept);
+  return warp_select_keep_stream(pool, n, keep, hist, kept);
 }
 
 }  // namespace curplsh_b200
