@@ -351,9 +351,11 @@ constexpr double kEstimateMuMin = 8.0;
 constexpr double kEstimateFailure = 1e-6;   // per-query failure probability for a uniform sample
 constexpr int kEstimateBlockRows = kHalfN;  // rows per block minimum (one epilogue warp's half tile)
 
+// The plan a search of this shape uses when the estimate is enabled (the
+// caller reads the process-wide switch once per search).
 EstimatePlan plan_estimate(int nq, long long n, int kp, int num_sms) {
   EstimatePlan e;
-  if (!g_bound_estimate.load(std::memory_order_relaxed) || nq < 1 || kp < 1) return e;
+  if (nq < 1 || kp < 1) return e;
   if (n < (1LL << 16) || n < 64LL * kp) return e;  // a short search gains too little
   const long long T = (n + kBN - 1) / kBN;
   long long tiles = (long long)std::ceil(kEstimateMuMax * (double)n / kp / kBN);
@@ -639,14 +641,16 @@ int do_search(curplsh_index* ix, int64_t num, const float* queries, int k, int p
   const bool i_dev = pointer_device(indices) == dev;
   const bool d_dev = pointer_device(distances) == dev;
   // A search that starts from an estimated bound checks it on the host (a
-  // failed query is searched again), so it always returns synchronised.
-  const bool est = ix->n > 0 && plan_estimate(nq, ix->n, kprime_for(form, k, rf, ix->n), ix->dres->num_sms).on;
+  // failed query is searched again), so it always returns synchronised.  The
+  // switch is read once here: planning and the check below agree.
+  const bool est = g_bound_estimate.load(std::memory_order_relaxed) && ix->n > 0 &&
+                   plan_estimate(nq, ix->n, kprime_for(form, k, rf, ix->n), ix->dres->num_sms).on;
   const bool sync = force_sync || est || !(q_dev && i_dev && d_dev);
 
   auto& slot = ix->ws[st];
   if (!slot) slot.reset(new StreamWorkspace());
   StreamWorkspace& w = *slot;
-  const size_t core = search_workspace_bytes(ix, nq, k, form, rf, true);
+  const size_t core = search_workspace_bytes(ix, nq, k, form, rf, est);
   const size_t qbytes = q_dev ? 0 : (size_t)nq * ix->dim * sizeof(float);
   const size_t obytes = (i_dev && d_dev) ? 0 : (size_t)nq * k * (sizeof(int) + sizeof(float));
   const size_t total = (size_t)round_up((long long)qbytes, 256) + (size_t)round_up((long long)obytes, 256) + core;
@@ -679,7 +683,7 @@ int do_search(curplsh_index* ix, int64_t num, const float* queries, int k, int p
   if (!q_dev)
     CUDA_TRY(cudaMemcpyAsync(const_cast<float*>(qd), queries, qbytes, cudaMemcpyDefault, st));
   int* fail = nullptr;
-  int rc = search_device(ix, nq, qd, k, form, rf, oi, od, st, base + off, &tm, true, &fail);
+  int rc = search_device(ix, nq, qd, k, form, rf, oi, od, st, base + off, &tm, est, &fail);
   if (rc) return rc;
   auto copy_out = [&]() -> int {
     if (!(i_dev && d_dev)) {
@@ -1079,7 +1083,7 @@ int curplsh_index_estimate_plan(curplsh_index* ix, int64_t num, int k, int preci
   *sample_rows = 0;
   *step = 1;
   *rank = 0;
-  if (ix->n == 0) return CURPLSH_OK;
+  if (ix->n == 0 || !g_bound_estimate.load(std::memory_order_relaxed)) return CURPLSH_OK;
   const EstimatePlan e = plan_estimate((int)num, ix->n, kprime_for(form, k, rf, ix->n), ix->dres->num_sms);
   if (e.on) {
     *sample_rows = e.rows;
