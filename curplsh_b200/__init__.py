@@ -134,6 +134,8 @@ def _load():
         "curplsh_index_estimate_plan": (i32, [vp, i64, i32, i32, i32, ctypes.POINTER(ctypes.c_int),
                                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
         "curplsh_index_get_fallback_count": (i32, [vp, ctypes.POINTER(ctypes.c_int64)]),
+        "curplsh_estimate_plan_shape": (i32, [i64, i64, i32, i32, ctypes.POINTER(ctypes.c_int),
+                                              ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -159,7 +161,7 @@ EXPORTED_SYMBOLS = (
     "curplsh_tuning_clear", "curplsh_server_config_init", "curplsh_server_create", "curplsh_server_submit",
     "curplsh_server_wait", "curplsh_server_get_stats", "curplsh_server_destroy", "curplsh_merge_shard_results",
     "curplsh_set_bound_estimate", "curplsh_get_bound_estimate", "curplsh_index_estimate_plan",
-    "curplsh_index_get_fallback_count",
+    "curplsh_index_get_fallback_count", "curplsh_estimate_plan_shape",
 )
 
 
@@ -493,6 +495,15 @@ def tuning_clear() -> None:
 def set_bound_estimate(enabled: bool) -> None:
     """Process-wide switch of the sampled bound estimate (speed only; results are identical)."""
     _check(_lib.curplsh_set_bound_estimate(1 if enabled else 0))
+
+
+def estimate_plan_shape(num_rows: int, num_queries: int, kprime: int, num_sms: int = 148):
+    """(sample_rows, step, rank) of the sampled bound estimate for a bare search shape
+    (no index or device needed); sample_rows == 0 when that shape uses none."""
+    a, b, c = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+    _check(_lib.curplsh_estimate_plan_shape(int(num_rows), int(num_queries), int(kprime), int(num_sms),
+                                            ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+    return a.value, b.value, c.value
 
 
 def get_bound_estimate() -> bool:

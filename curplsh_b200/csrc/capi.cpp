@@ -1093,6 +1093,24 @@ int curplsh_index_estimate_plan(curplsh_index* ix, int64_t num, int k, int preci
   return CURPLSH_OK;
 }
 
+int curplsh_estimate_plan_shape(int64_t num_rows, int64_t num_queries, int kprime, int num_sms, int* sample_rows,
+                                int* step, int* rank) {
+  if (!sample_rows || !step || !rank) return set_error(CURPLSH_ERR_INVALID_ARG, "null argument");
+  if (num_rows < 0 || num_rows > INT32_MAX || num_queries < 0 || num_queries > (int64_t)1 << 30 || kprime < 0 ||
+      num_sms < 1)
+    return set_error(CURPLSH_ERR_INVALID_ARG, "bad shape");
+  *sample_rows = 0;
+  *step = 1;
+  *rank = 0;
+  const EstimatePlan e = plan_estimate((int)num_queries, num_rows, kprime, num_sms);
+  if (e.on) {
+    *sample_rows = e.rows;
+    *step = e.step;
+    *rank = e.j;
+  }
+  return CURPLSH_OK;
+}
+
 int curplsh_index_get_fallback_count(curplsh_index* ix, int64_t* count) {
   if (!ix || !count) return set_error(CURPLSH_ERR_INVALID_ARG, "null argument");
   *count = ix->fallback_queries.load(std::memory_order_relaxed);

@@ -291,6 +291,11 @@ int curplsh_get_bound_estimate(int* enabled);
  * sample_rows / 128 block minima. */
 int curplsh_index_estimate_plan(curplsh_index* index, int64_t num_queries, int k, int precision,
                                 int rerank_factor, int* sample_rows, int* step, int* rank);
+/* The same plan for a bare shape (N rows, num_queries queries, k' candidates, num_sms SMs),
+ * without an index or a device: what any search of that shape would use while the switch is
+ * on. */
+int curplsh_estimate_plan_shape(int64_t num_rows, int64_t num_queries, int kprime, int num_sms, int* sample_rows,
+                                int* step, int* rank);
 /* Number of queries this index searched again after their estimate failed (since creation). */
 int curplsh_index_get_fallback_count(curplsh_index* index, int64_t* count);
 
