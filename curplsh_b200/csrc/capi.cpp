@@ -226,6 +226,7 @@ struct curplsh_index {
   bool bf16_exact = false;        // every stored value is exactly a BF16 value (rerank reads xh)
   long long generation = 0;       // bumped whenever the prepared database changes (add, reset)
   cudaEvent_t order_ev = nullptr; // orders default-stream searches after the legacy stream
+  cudaEvent_t fp8_ev = nullptr;   // recorded after the FP8 copy is written; every FP8 reader waits on it
   std::atomic<long long> fallback_queries{0};  // queries re-searched after an estimate failed
   std::map<cudaStream_t, std::unique_ptr<StreamWorkspace>> ws;
 
@@ -246,12 +247,21 @@ struct curplsh_index {
 
 namespace {
 
+// Builds the FP8 copy on `st` the first time a search needs it and makes `st`
+// wait for it.  The copy is written asynchronously, so a reader on any other
+// stream must wait on fp8_ev (recorded right after the write) before it reads
+// x8/xs; searches on `st` itself are ordered by the stream.
 int build_fp8(curplsh_index* ix, cudaStream_t st) {
-  if (ix->x8 || ix->n == 0) return CURPLSH_OK;
-  CUDA_TRY(cudaMalloc(&ix->x8, (size_t)ix->n_pad * ix->ld8));
-  CUDA_TRY(cudaMalloc(&ix->xs, (size_t)ix->n_pad * sizeof(float)));
-  CUDA_TRY(launch_prep_rows(ix->x32, ix->dim, (int)ix->n, ix->n_pad, ix->dim, nullptr, 0.f, nullptr, nullptr,
-                            ix->ld16, ix->x8, ix->xs, ix->ld8, st));
+  if (ix->n == 0) return CURPLSH_OK;
+  if (!ix->x8) {
+    CUDA_TRY(cudaMalloc(&ix->x8, (size_t)ix->n_pad * ix->ld8));
+    CUDA_TRY(cudaMalloc(&ix->xs, (size_t)ix->n_pad * sizeof(float)));
+    CUDA_TRY(launch_prep_rows(ix->x32, ix->dim, (int)ix->n, ix->n_pad, ix->dim, nullptr, 0.f, nullptr, nullptr,
+                              ix->ld16, ix->x8, ix->xs, ix->ld8, st));
+    CUDA_TRY(cudaEventRecord(ix->fp8_ev, st));
+    return CURPLSH_OK;
+  }
+  CUDA_TRY(cudaStreamWaitEvent(st, ix->fp8_ev, 0));
   return CURPLSH_OK;
 }
 
@@ -759,6 +769,7 @@ int index_lock_view(curplsh_index* ix, IndexView* v) {
   v->generation = ix->generation;
   v->bf16_exact = ix->bf16_exact;
   v->stream = ix->dres->def;
+  v->fp8_ready = ix->fp8_ev;
   return CURPLSH_OK;
 }
 void index_unlock(curplsh_index* ix) { ix->mu.unlock(); }
@@ -915,6 +926,7 @@ int curplsh_index_bf_create(curplsh_resources* r, int dim, const curplsh_bf_conf
   cudaError_t e = cudaMalloc(&ix->status, 2 * sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaMemset(ix->status, 0, 2 * sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ix->order_ev, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ix->fp8_ev, cudaEventDisableTiming);
   if (e != cudaSuccess) {
     cudaGetLastError();
     delete ix;
@@ -938,6 +950,7 @@ int curplsh_index_destroy(curplsh_index* ix) {
     ix->free_db();
     if (ix->status) cudaFree(ix->status);
     if (ix->order_ev) cudaEventDestroy(ix->order_ev);
+    if (ix->fp8_ev) cudaEventDestroy(ix->fp8_ev);
   }
   curplsh_resources* r = ix->res;
   delete ix;

@@ -234,6 +234,7 @@ struct IndexView {
   long long generation;  // changes whenever add()/reset() replace the prepared database
   bool bf16_exact;       // every stored value is exactly a BF16 value (xl is all zero)
   cudaStream_t stream;   // the index's default stream
+  cudaEvent_t fp8_ready; // recorded after the FP8 copy (x8, xs) was written; wait on it before reading them
 };
 // Locks the index (same lock as search/add) and fills `out`; unlock with index_unlock.
 int index_lock_view(curplsh_index* index, IndexView* out);

@@ -177,6 +177,16 @@ int search_noalloc_locked(const IndexView& v, int nq, const float* q, int k, int
   int* counts = reinterpret_cast<int*>(b + L.counts);
   uint64_t* pools = reinterpret_cast<uint64_t*>(b + L.pools);
 
+  // From the first enqueue on, an early return (a failed launch or copy) must
+  // not release the device lock while work that uses the scratch may still be
+  // in flight on `st`: the guard waits for the stream on every return path.
+  struct DrainOnReturn {
+    cudaStream_t st;
+    ~DrainOnReturn() { cudaStreamSynchronize(st); }
+  } drain{st};
+  // The FP8 copy is written asynchronously by the index's first regular FP8
+  // search, possibly on another stream: order this call after that write.
+  if (form == kFormFP8 && v.fp8_ready) NA_TRY(cudaStreamWaitEvent(st, v.fp8_ready, 0));
   // state that must start cleared on every call (the array keeps the last call's contents)
   NA_TRY(cudaMemsetAsync(status, 0, sizeof(uint32_t), st));
   NA_TRY(cudaMemsetAsync(qbound, 0xFF, (size_t)nq_pad * sizeof(uint32_t), st));
