@@ -176,7 +176,7 @@ def run_reference(args, world, rank):
     dev = "cuda" if torch.cuda.is_available() else "cpu"
     wl = args.workload if args.workload in WORKLOADS else WORKLOAD
     n_db, n_q, dim, _ = synth.CONFIGS[wl]
-    base, queries, k = synth.make(wl, device=dev)
+    base, queries, k = synth.make(wl, backend="torch", device=dev)
     base_h = base.cpu().numpy()
     q_h = queries.cpu().numpy()
     sample = 128
@@ -227,14 +227,14 @@ def run_batched(args, world, rank, local):
     precision = args.batch_form
     dbs = []
     for i, (n, d) in enumerate(dbs_spec):
-        x = synth.normal_bf16(n, d, seed=100 + i, device=dev)
+        x = synth.normal_bf16(n, d, seed=100 + i, backend="torch", device=dev)
         ix = cb.IndexBF(res, d, cb.IndexBFConfig(device=local, precision=precision))
         ix.add(n, x)
         dbs.append((ix, x))
     items = []
     for j, (db, nq, k) in enumerate(batches):
         ix, x = dbs[db]
-        q = synth.normal_bf16(nq, x.shape[1], seed=1000 + j + 7919 * rank, device=dev)
+        q = synth.normal_bf16(nq, x.shape[1], seed=1000 + j + 7919 * rank, backend="torch", device=dev)
         items.append((ix, q, k, torch.empty((nq, k), dtype=torch.int32, device=dev),
                       torch.empty((nq, k), dtype=torch.float32, device=dev)))
     torch.cuda.synchronize()  # the inputs were generated on torch's stream; the library uses its own
@@ -386,7 +386,7 @@ def run_serving(args, world, rank, local):
     torch.cuda.set_device(local)
     dev = f"cuda:{local}"
     n, d, k = args.serve_n, 256, 50
-    base, qpool = synth.mixture_bf16(n, 20000, d, device=dev)
+    base, qpool = synth.mixture_bf16(n, 20000, d, backend="torch", device=dev)
     torch.cuda.synchronize()
     res = cb.DeviceResources(local)
     ix = cb.IndexBF(res, d, cb.IndexBFConfig(device=local, precision=1))
@@ -536,7 +536,7 @@ def main():
     info = WORKLOADS[wl]
     n_db, _, dim, _ = synth.CONFIGS[wl]
     # every rank holds the same database and searches a full query batch (replicas)
-    base, queries, k = synth.make(wl, device=dev)
+    base, queries, k = synth.make(wl, backend="torch", device=dev)
     torch.cuda.synchronize()  # generated on torch's stream; the library orders its work on its own streams
     res = cb.DeviceResources(local)
     stream = torch.cuda.Stream(device=dev)
