@@ -126,11 +126,15 @@ def _load():
         "curplsh_server_create": (i32, [vp, ctypes.POINTER(_ServerCfg), ctypes.POINTER(vp)]),
         "curplsh_server_submit": (i32, [vp, i64, f32p, i32, i32p, f32p, ctypes.POINTER(ctypes.c_int64)]),
         "curplsh_server_wait": (i32, [vp, i64, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]),
+        "curplsh_server_wait_phases": (i32, [vp, i64, ctypes.c_double, ctypes.POINTER(ctypes.c_double),
+                                             ctypes.POINTER(ctypes.c_double)]),
         "curplsh_server_get_stats": (i32, [vp, ctypes.POINTER(_ServerStats)]),
         "curplsh_server_destroy": (i32, [vp]),
         "curplsh_merge_shard_results": (i32, [i64, i32, i32, f32p, i32p, vp, i32p, f32p, vp]),
         "curplsh_set_bound_estimate": (i32, [i32]),
         "curplsh_get_bound_estimate": (i32, [ctypes.POINTER(ctypes.c_int)]),
+        "curplsh_set_coarse_check": (i32, [i32]),
+        "curplsh_get_coarse_check": (i32, [ctypes.POINTER(ctypes.c_int)]),
         "curplsh_index_estimate_plan": (i32, [vp, i64, i32, i32, i32, ctypes.POINTER(ctypes.c_int),
                                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
         "curplsh_index_get_fallback_count": (i32, [vp, ctypes.POINTER(ctypes.c_int64)]),
@@ -159,9 +163,10 @@ EXPORTED_SYMBOLS = (
     "curplsh_search_l2_distance", "curplsh_index_search_noalloc", "curplsh_batch_create", "curplsh_batch_run",
     "curplsh_batch_get_info", "curplsh_batch_destroy", "curplsh_tuning_set", "curplsh_tuning_get",
     "curplsh_tuning_clear", "curplsh_server_config_init", "curplsh_server_create", "curplsh_server_submit",
-    "curplsh_server_wait", "curplsh_server_get_stats", "curplsh_server_destroy", "curplsh_merge_shard_results",
+    "curplsh_server_wait", "curplsh_server_wait_phases", "curplsh_server_get_stats", "curplsh_server_destroy", "curplsh_merge_shard_results",
     "curplsh_set_bound_estimate", "curplsh_get_bound_estimate", "curplsh_index_estimate_plan",
-    "curplsh_index_get_fallback_count", "curplsh_estimate_plan_shape",
+    "curplsh_index_get_fallback_count", "curplsh_estimate_plan_shape", "curplsh_set_coarse_check",
+    "curplsh_get_coarse_check",
 )
 
 
@@ -379,7 +384,8 @@ class IndexBF:
         return a.value, b.value, c.value
 
     def fallback_count(self) -> int:
-        """Queries searched again after their estimated bound failed (since creation)."""
+        """Queries searched again (since creation) after their estimated bound or their
+        coarse margin failed."""
         v = ctypes.c_int64()
         _check(_lib.curplsh_index_get_fallback_count(self._h, ctypes.byref(v)))
         return v.value
@@ -512,6 +518,19 @@ def get_bound_estimate() -> bool:
     return bool(v.value)
 
 
+def set_coarse_check(enabled: bool) -> None:
+    """Process-wide switch of the BF16/FP8 coarse-margin check: a query whose
+    candidate margin does not cover the coarse error seen among its candidates
+    is searched again in the FP32-exact form (on by default)."""
+    _check(_lib.curplsh_set_coarse_check(1 if enabled else 0))
+
+
+def get_coarse_check() -> bool:
+    v = ctypes.c_int(0)
+    _check(_lib.curplsh_get_coarse_check(ctypes.byref(v)))
+    return bool(v.value)
+
+
 class Server:
     """Serving loop with continuous batching over one resident index (no
     counterpart in the reference).  ``submit`` queues a request and returns a
@@ -549,6 +568,17 @@ class Server:
             self._keep.pop(ticket, None)
         _check(rc)
         return lat.value
+
+    def wait_phases(self, ticket: int, timeout: float = -1.0):
+        """wait() that also returns the latency's phases (seconds, host clock):
+        (latency, waiting for a step, step on the device, retiring)."""
+        lat = ctypes.c_double(0.0)
+        ph = (ctypes.c_double * 3)()
+        rc = _lib.curplsh_server_wait_phases(self._h, int(ticket), float(timeout), ctypes.byref(lat), ph)
+        if rc != ERR_STATE:
+            self._keep.pop(ticket, None)
+        _check(rc)
+        return lat.value, ph[0], ph[1], ph[2]
 
     def stats(self) -> dict:
         st = _ServerStats()

@@ -203,6 +203,10 @@ struct StreamWorkspace {
 // Library-wide switch of the sampled bound estimate (results are identical
 // either way; it only changes speed).
 std::atomic<int> g_bound_estimate{1};
+// Library-wide switch of the coarse-margin check of the BF16/FP8 forms (a
+// query whose candidates the coarse distances cannot vouch for is searched
+// again in the exact form; see merge_rerank.cu).
+std::atomic<int> g_coarse_check{1};
 }  // namespace
 
 struct curplsh_index {
@@ -392,9 +396,17 @@ struct SearchShape {
   long long nq_pad = 0;
   size_t pool_lists = 0;
   EstimatePlan est;
+  bool coarse = false;  // the merge checks the coarse margin (needs the failure list)
 };
 
-SearchShape search_shape(const curplsh_index* ix, int nq, int k, int form, int rerank_factor, bool allow_est) {
+// Whether a search of this form checks the coarse margin (the switch is read
+// once per search by the caller and passed down).
+bool coarse_check_applies(const curplsh_index* ix, int form, int kp, bool enabled) {
+  return enabled && form != kFormExact && ix->n > 0 && kp < ix->n;
+}
+
+SearchShape search_shape(const curplsh_index* ix, int nq, int k, int form, int rerank_factor, bool allow_est,
+                         bool coarse_on) {
   SearchShape sh;
   sh.kp = kprime_for(form, k, rerank_factor, ix->n);
   const TuneParams tp = tune_lookup(form, ix->dim, k, nq);
@@ -403,6 +415,7 @@ SearchShape search_shape(const curplsh_index* ix, int nq, int k, int form, int r
   sh.nq_pad = round_up(nq, kBM);
   sh.pool_lists = (size_t)sh.plan.num_qblocks * kBM * sh.plan.units_per_block;
   if (allow_est) sh.est = plan_estimate(nq, ix->n, sh.kp, ix->dres->num_sms);
+  sh.coarse = coarse_check_applies(ix, form, sh.kp, coarse_on);
   return sh;
 }
 
@@ -424,10 +437,8 @@ size_t carve_search(Carve& c, const curplsh_index* ix, const SearchShape& sh, in
   b->qn = c.take<float>(sh.nq_pad);
   b->qs = c.take<float>(sh.nq_pad);
   b->qbound = c.take<uint32_t>(sh.nq_pad);
-  if (sh.est.on) {
-    b->minima = c.take<float>((size_t)sh.nq_pad * sh.est.blocks);
-    b->fail = c.take<int>(1 + (size_t)nq);
-  }
+  if (sh.est.on) b->minima = c.take<float>((size_t)sh.nq_pad * sh.est.blocks);
+  if (sh.est.on || sh.coarse) b->fail = c.take<int>(1 + (size_t)nq);
   b->counts = c.take<int>(sh.pool_lists);
   b->pools = c.take<uint64_t>(sh.pool_lists * (size_t)sh.P);
   return (size_t)round_up((long long)c.off, 256);
@@ -472,11 +483,13 @@ cudaError_t fused_stats_print(const char* label, const FusedLaunch& f, cudaStrea
 #endif
 
 // The search proper.  Device-side inputs/outputs; `st` orders everything.
-// With `allow_est` a sampled bound estimate may be used; then *fail_out
-// points at the device list of queries it failed ([0] count, then indices),
-// which the caller must search again (else *fail_out is null).
+// With `allow_est` a sampled bound estimate may be used, with `coarse_on` the
+// BF16/FP8 forms check their coarse margin; when either applies, *fail_out
+// points at the device list of queries that failed a check ([0] count, then
+// indices), which the caller must search again (else *fail_out is null).
 int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form, int rerank_factor, int* out_idx,
-                  float* out_dist, cudaStream_t st, char* extra_base, Timing* tm, bool allow_est, int** fail_out) {
+                  float* out_dist, cudaStream_t st, char* extra_base, Timing* tm, bool allow_est, bool coarse_on,
+                  int** fail_out) {
   const int d = ix->dim;
   *fail_out = nullptr;
   if (ix->n == 0) {
@@ -487,7 +500,7 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
     int rc = build_fp8(ix, st);
     if (rc) return rc;
   }
-  const SearchShape sh = search_shape(ix, nq, k, form, rerank_factor, allow_est);
+  const SearchShape sh = search_shape(ix, nq, k, form, rerank_factor, allow_est, coarse_on);
   const int kp = sh.kp, P = sh.P;
   const FusedPlan& plan = sh.plan;
   const long long nq_pad = sh.nq_pad;
@@ -533,7 +546,6 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
     e.kprime = 1;
     e.minima = b.minima;
     e.plan = sh.est.plan;
-    CUDA_TRY(cudaMemsetAsync(b.fail, 0, sizeof(int), st));
 #ifdef CURPLSH_FUSED_STATS
     CUDA_TRY(fused_stats_begin(&e, st));
 #endif
@@ -546,6 +558,7 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
   } else {
     CUDA_TRY(cudaMemsetAsync(b.qbound, 0xFF, (size_t)nq_pad * sizeof(uint32_t), st));
   }
+  if (b.fail) CUDA_TRY(cudaMemsetAsync(b.fail, 0, sizeof(int), st));
   tm->rec(2, st);
 #ifdef CURPLSH_FUSED_STATS
   CUDA_TRY(fused_stats_begin(&f, st));
@@ -566,7 +579,8 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
   m.pools = b.pools;
   m.pool_counts = b.counts;
   m.q_bound = b.qbound;
-  if (sh.est.on) {
+  m.checks = (sh.est.on ? kCheckEstimate : 0) | (sh.coarse ? kCheckCoarse : 0);
+  if (m.checks) {
     m.fail_count = b.fail;
     m.fail_list = b.fail + 1;
   }
@@ -582,27 +596,29 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
   m.status = ix->status;
   CUDA_TRY(launch_merge_rerank(m, st));
   tm->rec(4, st);
-  if (sh.est.on) *fail_out = b.fail;
+  if (m.checks) *fail_out = b.fail;
   return CURPLSH_OK;
 }
 
 size_t search_workspace_bytes(const curplsh_index* ix, int nq, int k, int form, int rerank_factor,
-                              bool allow_est) {
+                              bool allow_est, bool coarse_on) {
   if (ix->n == 0) return 0;
-  const SearchShape sh = search_shape(ix, nq, k, form, rerank_factor, allow_est);
+  const SearchShape sh = search_shape(ix, nq, k, form, rerank_factor, allow_est, coarse_on);
   Carve c(nullptr);
   SearchBufs b;
   return carve_search(c, ix, sh, nq, form, &b) + 256;
 }
 
-// Searches again, without an estimate, the `nf` queries listed at fail_dev + 1
-// (device) and writes their results into the full result arrays.
-int search_failed(curplsh_index* ix, int nf, const int* fail_dev, const float* q_dev, int k, int form,
-                  int rerank_factor, int* out_idx, float* out_dist, cudaStream_t st, StreamWorkspace& w) {
+// Searches again the `nf` queries listed at fail_dev + 1 (device) -- in the
+// exact form, without an estimate, so no check applies -- and writes their
+// results into the full result arrays.
+int search_failed(curplsh_index* ix, int nf, const int* fail_dev, const float* q_dev, int k, int rerank_factor,
+                  int* out_idx, float* out_dist, cudaStream_t st, StreamWorkspace& w) {
   const int d = ix->dim;
+  const int form = kFormExact;
   const size_t qbytes = (size_t)round_up((long long)nf * d * sizeof(float), 256);
   const size_t obytes = (size_t)round_up((long long)nf * k * (sizeof(int) + sizeof(float)), 256);
-  const size_t core = search_workspace_bytes(ix, nf, k, form, rerank_factor, false);
+  const size_t core = search_workspace_bytes(ix, nf, k, form, rerank_factor, false, false);
   cudaError_t e = w.fb.ensure(qbytes + obytes + core);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -617,7 +633,7 @@ int search_failed(curplsh_index* ix, int nf, const int* fail_dev, const float* q
   Timing none;
   int* again = nullptr;
   int rc = search_device(ix, nf, qf, k, form, rerank_factor, oif, odf, st, base + qbytes + obytes, &none, false,
-                         &again);
+                         false, &again);
   if (rc) return rc;
   CUDA_TRY(launch_scatter_results(oif, odf, fail_dev + 1, nf, k, out_idx, out_dist, st));
   ix->fallback_queries.fetch_add(nf, std::memory_order_relaxed);
@@ -653,14 +669,18 @@ int do_search(curplsh_index* ix, int64_t num, const float* queries, int k, int p
   // A search that starts from an estimated bound checks it on the host (a
   // failed query is searched again), so it always returns synchronised.  The
   // switch is read once here: planning and the check below agree.
+  const int kp = ix->n > 0 ? kprime_for(form, k, rf, ix->n) : 0;
   const bool est = g_bound_estimate.load(std::memory_order_relaxed) && ix->n > 0 &&
-                   plan_estimate(nq, ix->n, kprime_for(form, k, rf, ix->n), ix->dres->num_sms).on;
-  const bool sync = force_sync || est || !(q_dev && i_dev && d_dev);
+                   plan_estimate(nq, ix->n, kp, ix->dres->num_sms).on;
+  // Likewise the coarse-margin check of the BF16/FP8 forms: a query it lists
+  // is searched again in the exact form before the call returns.
+  const bool coarse = coarse_check_applies(ix, form, kp, g_coarse_check.load(std::memory_order_relaxed) != 0);
+  const bool sync = force_sync || est || coarse || !(q_dev && i_dev && d_dev);
 
   auto& slot = ix->ws[st];
   if (!slot) slot.reset(new StreamWorkspace());
   StreamWorkspace& w = *slot;
-  const size_t core = search_workspace_bytes(ix, nq, k, form, rf, est);
+  const size_t core = search_workspace_bytes(ix, nq, k, form, rf, est, coarse);
   const size_t qbytes = q_dev ? 0 : (size_t)nq * ix->dim * sizeof(float);
   const size_t obytes = (i_dev && d_dev) ? 0 : (size_t)nq * k * (sizeof(int) + sizeof(float));
   const size_t total = (size_t)round_up((long long)qbytes, 256) + (size_t)round_up((long long)obytes, 256) + core;
@@ -693,7 +713,7 @@ int do_search(curplsh_index* ix, int64_t num, const float* queries, int k, int p
   if (!q_dev)
     CUDA_TRY(cudaMemcpyAsync(const_cast<float*>(qd), queries, qbytes, cudaMemcpyDefault, st));
   int* fail = nullptr;
-  int rc = search_device(ix, nq, qd, k, form, rf, oi, od, st, base + off, &tm, est, &fail);
+  int rc = search_device(ix, nq, qd, k, form, rf, oi, od, st, base + off, &tm, est, coarse, &fail);
   if (rc) return rc;
   auto copy_out = [&]() -> int {
     if (!(i_dev && d_dev)) {
@@ -714,8 +734,9 @@ int do_search(curplsh_index* ix, int64_t num, const float* queries, int k, int p
     uint32_t s = hw[0];
     const int nf = (int)hw[1];
     if (!s && nf > 0) {
-      // queries whose estimated bound was too small: search them again
-      rc = search_failed(ix, nf, fail, qd, k, form, rf, oi, od, st, w);
+      // queries whose estimated bound was too small, or whose coarse margin
+      // failed: search them again in the exact form
+      rc = search_failed(ix, nf, fail, qd, k, rf, oi, od, st, w);
       if (rc) return rc;
       rc = copy_out();
       if (rc) return rc;
@@ -1081,6 +1102,17 @@ int curplsh_set_bound_estimate(int enabled) {
 int curplsh_get_bound_estimate(int* enabled) {
   if (!enabled) return set_error(CURPLSH_ERR_INVALID_ARG, "null argument");
   *enabled = g_bound_estimate.load(std::memory_order_relaxed);
+  return CURPLSH_OK;
+}
+
+int curplsh_set_coarse_check(int enabled) {
+  g_coarse_check.store(enabled ? 1 : 0, std::memory_order_relaxed);
+  return CURPLSH_OK;
+}
+
+int curplsh_get_coarse_check(int* enabled) {
+  if (!enabled) return set_error(CURPLSH_ERR_INVALID_ARG, "null argument");
+  *enabled = g_coarse_check.load(std::memory_order_relaxed);
   return CURPLSH_OK;
 }
 

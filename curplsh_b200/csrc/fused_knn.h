@@ -154,8 +154,13 @@ cudaError_t launch_prep_segments(PrepSegment* segs, int n, int d, long long ld16
 // Plain squared (or not) L2 norms, as computeL2Norm.
 cudaError_t launch_l2_norms(const float* x, long long n, int d, float* norms, int squared, cudaStream_t st);
 
+// Checks of the merge pass that list a query for a search again (MergeItem::checks).
+constexpr int kCheckEstimate = 1;  // the fused pass started from estimated bounds: verify them
+constexpr int kCheckCoarse = 2;    // coarse (BF16/FP8) distances: verify the candidate margin
+
 struct MergeLaunch {
   int nq, nb, d, k, kprime, pool_cap;
+  int checks = 0;                // kCheck* bits; any bit needs fail_count / fail_list
   FusedPlan plan;
   const uint64_t* pools;
   const int* pool_counts;
@@ -188,9 +193,15 @@ struct MergeItem {
   const uint64_t* pools;   // the fused item's pools and counts
   const int* pool_counts;
   const uint32_t* q_bound;       // the fused item's final bounds by pool row (may be null)
-  // Non-null when the fused pass started from estimated bounds: a query with
-  // fewer than k' candidates under its final bound may miss rows, so its
-  // index within the item is appended to fail_list (count in *fail_count).
+  // kCheck* bits.  kCheckEstimate: the fused pass started from estimated
+  // bounds, and a query with fewer than k' candidates under its final bound
+  // may miss rows.  kCheckCoarse: the candidates were chosen by coarse
+  // (BF16/FP8) distances, and a query whose candidate margin does not cover
+  // the coarse error seen among its candidates may miss rows.  Either way the
+  // query's index within the item is appended to fail_list (count in
+  // *fail_count) for a search again.
+  int checks;
+  long long nb_total;      // database rows (kCheckCoarse: nothing to check when k' covers them all)
   int* fail_count;
   int* fail_list;
   const float* queries;    // [nq x d] fp32, row stride d

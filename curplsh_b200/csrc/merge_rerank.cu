@@ -132,6 +132,9 @@ __global__ void __launch_bounds__(kMergeThreads) merge_rerank_kernel(const __gri
   if (tid == 0) {
     misc[0] = 0;
     misc[4] = 0;
+    misc[5] = 0u;            // max over candidates of (coarse - exact), order bits
+    misc[6] = 0xFFFFFFFFu;   // min of the same
+    misc[7] = 0u;            // largest coarse distance among the candidates, order bits
   }
   for (int l = tid; l < nlists; l += kMergeThreads) lcnt[l] = m.pool_counts[list0 + l];
   __syncthreads();
@@ -164,7 +167,8 @@ __global__ void __launch_bounds__(kMergeThreads) merge_rerank_kernel(const __gri
   // the whole database are among the candidates (their k'-th is then <= E, and
   // a pool selection never drops one of them).  Fewer: E may have been too
   // small, and the query is listed for a search without the estimate.
-  if (m.fail_count && cnt < m.kprime && tid == 0) {
+  const bool listed = (m.checks & kCheckEstimate) && cnt < m.kprime;  // each query is listed at most once
+  if (listed && tid == 0) {
     const int pos = atomicAdd(m.fail_count, 1);
     m.fail_list[pos] = q;
   }
@@ -276,6 +280,19 @@ __global__ void __launch_bounds__(kMergeThreads) merge_rerank_kernel(const __gri
       s1 += __shfl_xor_sync(0xffffffffu, s1, o);
     }
     if (lane == 0) {
+      if (m.checks & kCheckCoarse) {
+        const float c0 = ord2f((uint32_t)(cand[c] >> 32));
+        float emax = c0 - s0, emin = c0 - s0, cmax = c0;
+        if (two) {
+          const float c1 = ord2f((uint32_t)(cand[c + 1] >> 32));
+          emax = fmaxf(emax, c1 - s1);
+          emin = fminf(emin, c1 - s1);
+          cmax = fmaxf(cmax, c1);
+        }
+        atomicMax(&misc[5], f2ord(emax));
+        atomicMin(&misc[6], f2ord(emin));
+        atomicMax(&misc[7], f2ord(cmax));
+      }
       cand[c] = make_key(s0, i0);
       if (two) cand[c + 1] = make_key(s1, i1);
     }
@@ -298,6 +315,25 @@ __global__ void __launch_bounds__(kMergeThreads) merge_rerank_kernel(const __gri
         }
       }
       __syncthreads();
+    }
+  }
+  // Coarse-margin check.  Every row that is not a candidate has a coarse key
+  // above the largest candidate's, cmax.  With e = coarse - exact, such a row
+  // can come before the k-th exact result D_k only if its e exceeds
+  // cmax - D_k.  The candidates' own errors span [emin, emax]; a query passes
+  // when cmax - D_k >= emax + (emax - emin), i.e. a row outside the
+  // candidates would need an error beyond the largest seen by a further full
+  // spread.  This is a check of the data against the form's precision, not a
+  // proof: it lists queries whose data is too fine for the coarse form (e.g.
+  // FP8 on integer-valued rows) for an exact search again.  Exact coarse
+  // distances (spread 0) always pass, since then D_k <= cmax.
+  if ((m.checks & kCheckCoarse) && !listed && tid == 0 && kept >= m.kprime && kept > m.k &&
+      m.kprime < m.nb_total) {
+    const float emax = ord2f(misc[5]), emin = ord2f(misc[6]), cmax = ord2f(misc[7]);
+    const float dk = ord2f((uint32_t)(cand[m.k - 1] >> 32));
+    if (!(cmax - dk >= emax + (emax - emin))) {
+      const int pos = atomicAdd(m.fail_count, 1);
+      m.fail_list[pos] = q;
     }
   }
   for (int t = tid; t < m.k; t += kMergeThreads) {
@@ -357,7 +393,7 @@ cudaError_t launch_merge_batch(MergeItem* items, int n, int d, uint32_t* status,
     len = std::min<long long>(len, items[i].num_tiles);
     bounded = bounded || (items[i].q_bound && len * kBN >= items[i].kprime);
     // the estimate check counts the keys under the final bound
-    bounded = bounded || (items[i].q_bound && items[i].fail_count);
+    bounded = bounded || (items[i].q_bound && (items[i].checks & kCheckEstimate));
   }
   a.pre_cap = bounded ? 2 * kp2 : 0;
   a.lcnt_n = (umax + 3) & ~3;
@@ -390,6 +426,8 @@ cudaError_t launch_merge_rerank(const MergeLaunch& m, cudaStream_t st) {
   it.pools = m.pools;
   it.pool_counts = m.pool_counts;
   it.q_bound = m.q_bound;
+  it.checks = m.checks;
+  it.nb_total = m.nb;
   it.fail_count = m.fail_count;
   it.fail_list = m.fail_list;
   it.queries = m.queries;

@@ -126,7 +126,9 @@ struct Request {
   int32_t* indices = nullptr;
   float* distances = nullptr;
   bool q_dev = false, o_dev = false;
-  double t_submit = 0, t_done = 0;
+  // host clock: submitted, issued in a step, the step's completion callback
+  // ran, results visible to wait()
+  double t_submit = 0, t_issue = 0, t_gpu = 0, t_done = 0;
   int state = kPending;
   int err = CURPLSH_OK;
   std::string msg;
@@ -149,6 +151,7 @@ struct Step {
   // host-output copies to do at completion: (ticket, pinned offset)
   std::vector<std::pair<int64_t, size_t>> host_out;
   std::atomic<bool> finished{false};
+  double t_gpu_done = 0;  // host clock when the completion callback ran
 };
 
 }  // namespace
@@ -182,6 +185,7 @@ namespace {
 // wake-up fell between its check and its wait.
 void CUDART_CB on_step_done(void* p) {
   Step* s = static_cast<Step*>(p);
+  s->t_gpu_done = now_s();
   s->finished.store(true);
   s->srv->cv_work.notify_one();
 }
@@ -236,6 +240,7 @@ void finish_step(curplsh_server* s, Step& st) {
   for (int64_t tk : st.tickets) {
     Request& r = s->reqs[tk];
     r.t_done = t;
+    r.t_gpu = st.t_gpu_done;
     if (status) {
       r.state = kFailed;
       r.err = CURPLSH_ERR_DEVICE;
@@ -306,7 +311,11 @@ bool issue_step(curplsh_server* s, std::unique_lock<std::mutex>& lk) {
     return true;
   }
   for (size_t i = 0; i < take.size(); ++i) s->pending.pop_front();
-  for (int64_t t : take) s->reqs[t].state = kRunning;
+  const double t_issue = now_s();
+  for (int64_t t : take) {
+    s->reqs[t].state = kRunning;
+    s->reqs[t].t_issue = t_issue;
+  }
   st->tickets = take;
   slot.busy = true;
   // ---- bind memory: [plan][staging...]; host inputs go through the pinned slot buffer
@@ -545,7 +554,8 @@ int curplsh_server_submit(curplsh_server* s, int64_t num, const float* queries, 
   return CURPLSH_OK;
 }
 
-int curplsh_server_wait(curplsh_server* s, int64_t ticket, double timeout_s, double* latency_s) {
+int curplsh_server_wait_phases(curplsh_server* s, int64_t ticket, double timeout_s, double* latency_s,
+                               double* phases) {
   if (!s) return fail(CURPLSH_ERR_INVALID_ARG, "null server");
   std::unique_lock<std::mutex> lk(s->mu);
   auto it = s->reqs.find(ticket);
@@ -559,8 +569,18 @@ int curplsh_server_wait(curplsh_server* s, int64_t ticket, double timeout_s, dou
   const Request r = it->second;
   s->reqs.erase(it);
   if (latency_s) *latency_s = r.t_done - r.t_submit;
+  if (phases) {
+    const bool ran = r.t_issue > 0 && r.t_gpu > 0;
+    phases[0] = r.t_issue > 0 ? r.t_issue - r.t_submit : r.t_done - r.t_submit;  // waiting for a step
+    phases[1] = ran ? r.t_gpu - r.t_issue : 0.0;                                 // step issued -> GPU done
+    phases[2] = ran ? r.t_done - r.t_gpu : 0.0;                                  // GPU done -> visible
+  }
   if (r.state == kFailed) return fail(r.err ? r.err : CURPLSH_ERR_DEVICE, "%s", r.msg.c_str());
   return CURPLSH_OK;
+}
+
+int curplsh_server_wait(curplsh_server* s, int64_t ticket, double timeout_s, double* latency_s) {
+  return curplsh_server_wait_phases(s, ticket, timeout_s, latency_s, nullptr);
 }
 
 int curplsh_server_get_stats(curplsh_server* s, curplsh_server_stats* out) {

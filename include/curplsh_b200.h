@@ -244,6 +244,11 @@ int curplsh_server_submit(curplsh_server* server, int64_t num, const float* quer
  * returns its status and, when latency_s is not NULL, seconds from submit to completion.  A ticket
  * can be waited for once. */
 int curplsh_server_wait(curplsh_server* server, int64_t ticket, double timeout_s, double* latency_s);
+/* curplsh_server_wait that also splits the latency (host clock) into phases[3]: waiting for a
+ * step (submit to issue), the step on the device (issue to its completion callback), and
+ * retiring (callback to the results being visible to wait).  No counterpart in the reference. */
+int curplsh_server_wait_phases(curplsh_server* server, int64_t ticket, double timeout_s, double* latency_s,
+                               double* phases);
 int curplsh_server_get_stats(curplsh_server* server, curplsh_server_stats* out);
 /* Finishes every queued request, then frees the server. */
 int curplsh_server_destroy(curplsh_server* server);
@@ -296,8 +301,24 @@ int curplsh_index_estimate_plan(curplsh_index* index, int64_t num_queries, int k
  * on. */
 int curplsh_estimate_plan_shape(int64_t num_rows, int64_t num_queries, int kprime, int num_sms, int* sample_rows,
                                 int* step, int* rank);
-/* Number of queries this index searched again after their estimate failed (since creation). */
+/* Number of queries this index searched again (since creation) because their estimate or their
+ * coarse margin (below) failed. */
 int curplsh_index_get_fallback_count(curplsh_index* index, int64_t* count);
+
+/* ------------------------------------------------------------ coarse-margin check */
+/* No counterpart in the reference.  The BF16 and FP8 forms pick k' candidates by coarse
+ * distances and rerank them exactly; rows outside the candidates are never looked at again.
+ * With the check on, the merge pass compares, per query, the margin between the largest
+ * candidate coarse distance and the k-th exact result with the coarse errors (coarse - exact)
+ * of the candidates themselves: when the margin is smaller than the largest error plus the
+ * errors' spread, the coarse form is too coarse for this query's data and the query is searched
+ * again in the FP32-exact form before the call returns (counted by
+ * curplsh_index_get_fallback_count).  Forms whose coarse distances are exact for the data (BF16
+ * on integer or BF16-valued rows) always pass.  It is a check of the data against the form's
+ * precision, not a proof.  Applies to curplsh_index_search / _ex / _profiled; a search that uses
+ * it returns synchronised even with device buffers.  Process-wide; on (1) by default. */
+int curplsh_set_coarse_check(int enabled);
+int curplsh_get_coarse_check(int* enabled);
 
 #ifdef __cplusplus
 } /* extern "C" */

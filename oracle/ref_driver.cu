@@ -31,7 +31,6 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
-#include <memory>
 #include <string>
 
 #include "device_resources.h"
@@ -55,7 +54,10 @@ int cuda_fail(const char* what, cudaError_t e) {
   return 2;
 }
 
-std::unique_ptr<curplsh::DeviceResources> g_res;
+// Never destroyed: the reference's destructor checks CUDA calls and exits the
+// process on an error, and at process exit the CUDA runtime is already
+// unloading (cudaErrorCudartUnloading).  The process's end releases it.
+curplsh::DeviceResources* g_res = nullptr;
 int g_dev = -1;
 
 struct RefDatabase {
@@ -81,7 +83,7 @@ int curplsh_ref_open(int device) {
   if (g_res) return g_dev == device ? 0 : fail("curplsh_ref_open: already open on another device");
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) return cuda_fail("cudaSetDevice", e);
-  g_res.reset(new curplsh::DeviceResources());
+  g_res = new curplsh::DeviceResources();
   g_res->initializeForDevice(device);
   g_dev = device;
   return 0;
@@ -150,7 +152,7 @@ int curplsh_ref_search(void* h, const float* queries, int64_t nq, int k, int* in
     e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cuda_fail("sync", e);
     const double t1 = now_ms();
-    curplsh::searchL2Distance(g_res.get(), db->data, &db->norms, q, k, idx, dist, true);
+    curplsh::searchL2Distance(g_res, db->data, &db->norms, q, k, idx, dist, true);
     e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return cuda_fail("searchL2Distance", e);
     const double t2 = now_ms();

@@ -56,3 +56,40 @@ def assert_knn_matches(base, queries, got_d, got_i, ref_d, ref_i, min_recall=1.0
         bad = sep & (got_i != ref_i)
         assert not bad.any(), f"{int(bad.sum())} well-separated positions differ, first at {np.argwhere(bad)[0]}"
     return rec
+
+
+def assert_matches_reference(got_d, got_i, ref_d, ref_i, sep_rtol=SEP_RTOL, dist_rtol=DIST_RTOL):
+    """Compare a result with the reference's own output (cuRPLSH
+    searchL2Distance with exact distances), rank by rank.
+
+    The reference computes ||q||^2 + ||x||^2 - 2 q.x in FP32 and breaks ties in
+    no particular order, so: distances must agree within `dist_rtol` at every
+    rank; indices must be equal wherever the reference's distance at that rank
+    is separated from both neighbours by more than `sep_rtol` (relative); and,
+    per query, the set of indices strictly inside the k-th distance's tie group
+    (distance below kth * (1 - sep_rtol)) must be the same set.  Returns the
+    number of positions compared strictly."""
+    got_d = np.asarray(got_d, np.float64)
+    got_i = np.asarray(got_i, np.int64)
+    ref_d = np.asarray(ref_d, np.float64)
+    ref_i = np.asarray(ref_i, np.int64)
+    assert got_d.shape == ref_d.shape and got_i.shape == ref_i.shape, (got_d.shape, ref_d.shape)
+    nq, k = ref_i.shape
+    err = np.abs(got_d - ref_d)
+    lim = dist_rtol * np.abs(ref_d) + 1e-6 * max(float(np.mean(np.abs(ref_d))), 1e-30)
+    assert (err <= lim).all(), f"distance differs from the reference by {err.max():.3e} at {np.unravel_index(np.argmax(err - lim), err.shape)}"
+    gap = sep_rtol * np.abs(ref_d)
+    lo = np.concatenate([np.full((nq, 1), -np.inf), ref_d[:, :-1]], axis=1)
+    hi = np.concatenate([ref_d[:, 1:], np.full((nq, 1), np.inf)], axis=1)
+    sep = ((ref_d - lo) > gap) & ((hi - ref_d) > gap)
+    # the last rank is compared only if it is separated from the reference's
+    # (unknown) k+1-th distance, which the inside-set rule below covers instead
+    sep[:, -1] = False
+    bad = sep & (got_i != ref_i)
+    assert not bad.any(), f"{int(bad.sum())} separated positions differ from the reference, first {np.argwhere(bad)[0]}"
+    for q in range(nq):
+        thr = ref_d[q, -1] * (1 - sep_rtol) if ref_d[q, -1] > 0 else -np.inf
+        a = set(ref_i[q][ref_d[q] < thr].tolist())
+        b = set(got_i[q][got_d[q] < thr].tolist())
+        assert a == b, f"query {q}: indices inside the k-th distance differ from the reference ({sorted(a ^ b)[:5]})"
+    return int(sep.sum())
