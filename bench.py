@@ -289,7 +289,7 @@ def run_single(cb, synth, wl, args, world, rank, local, res, peaks, fp8_peak, wi
         ix = cb.IndexBF(res, dim, cb.IndexBFConfig(device=local, precision=form))
         ix.add(n_db, base)
         indexes[form] = ix
-        fb0 = ix.fallback_count()
+        fb0, cf0 = ix.fallback_count(), ix.coarse_fallback_count()
         ix.search_ex(Q, queries, k, oi, od, stream=stream)
         stream.synchronize()
         if rank == 0 and not args.no_recall:
@@ -298,7 +298,8 @@ def run_single(cb, synth, wl, args, world, rank, local, res, peaks, fp8_peak, wi
             rec, _ = oracle.recall_at_k(base_h, qs_h, gi, rd[:, :k])
             err = float(np.max(np.abs(gd - rd[:, :k]) / np.maximum(np.abs(rd[:, :k]), 1e-30)))
             form_results[FORMS[form]] = {"recall_at_k": rec, "max_rel_dist_err": err,
-                                         "queries_searched_again": ix.fallback_count() - fb0}
+                                         "estimate_failed_queries": ix.fallback_count() - fb0,
+                                         "coarse_check_failed_queries": ix.coarse_fallback_count() - cf0}
 
     # ---- timed region: device-resident queries, CUDA events on our stream
     flops = 2.0 * Q * n_db * dim
@@ -324,9 +325,9 @@ def run_single(cb, synth, wl, args, world, rank, local, res, peaks, fp8_peak, wi
         sampler = ClockSampler(local) if (with_clocks and form == headline) else None
         if sampler:
             sampler.__enter__()
-        fb0 = ix.fallback_count()
+        fb0 = ix.fallback_count() + ix.coarse_fallback_count()
         ms = timed_searches(ix, args.steps)
-        fb = ix.fallback_count() - fb0
+        fb = ix.fallback_count() + ix.coarse_fallback_count() - fb0
         if sampler:
             sampler.__exit__(None, None, None)
             clocks = sampler.summary()

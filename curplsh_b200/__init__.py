@@ -134,6 +134,7 @@ def _load():
         "curplsh_set_bound_estimate": (i32, [i32]),
         "curplsh_get_bound_estimate": (i32, [ctypes.POINTER(ctypes.c_int)]),
         "curplsh_set_coarse_check": (i32, [i32]),
+        "curplsh_index_get_coarse_fallback_count": (i32, [vp, ctypes.POINTER(ctypes.c_int64)]),
         "curplsh_get_coarse_check": (i32, [ctypes.POINTER(ctypes.c_int)]),
         "curplsh_index_estimate_plan": (i32, [vp, i64, i32, i32, i32, ctypes.POINTER(ctypes.c_int),
                                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
@@ -166,7 +167,7 @@ EXPORTED_SYMBOLS = (
     "curplsh_server_wait", "curplsh_server_wait_phases", "curplsh_server_get_stats", "curplsh_server_destroy", "curplsh_merge_shard_results",
     "curplsh_set_bound_estimate", "curplsh_get_bound_estimate", "curplsh_index_estimate_plan",
     "curplsh_index_get_fallback_count", "curplsh_estimate_plan_shape", "curplsh_set_coarse_check",
-    "curplsh_get_coarse_check",
+    "curplsh_get_coarse_check", "curplsh_index_get_coarse_fallback_count",
 )
 
 
@@ -384,10 +385,16 @@ class IndexBF:
         return a.value, b.value, c.value
 
     def fallback_count(self) -> int:
-        """Queries searched again (since creation) after their estimated bound or their
-        coarse margin failed."""
+        """Queries searched again after their estimated bound failed (since creation)."""
         v = ctypes.c_int64()
         _check(_lib.curplsh_index_get_fallback_count(self._h, ctypes.byref(v)))
+        return v.value
+
+    def coarse_fallback_count(self) -> int:
+        """Queries searched again in the exact form after their coarse margin failed
+        (since creation)."""
+        v = ctypes.c_int64()
+        _check(_lib.curplsh_index_get_coarse_fallback_count(self._h, ctypes.byref(v)))
         return v.value
 
     # -- convenience forms

@@ -232,6 +232,7 @@ struct curplsh_index {
   cudaEvent_t order_ev = nullptr; // orders default-stream searches after the legacy stream
   cudaEvent_t fp8_ev = nullptr;   // recorded after the FP8 copy is written; every FP8 reader waits on it
   std::atomic<long long> fallback_queries{0};  // queries re-searched after an estimate failed
+  std::atomic<long long> coarse_queries{0};    // queries re-searched after their coarse margin failed
   std::map<cudaStream_t, std::unique_ptr<StreamWorkspace>> ws;
 
   void free_db() {
@@ -333,14 +334,6 @@ struct Timing {
 // k' candidates lie under the final bound, the k' nearest rows are among them
 // (see merge_rerank.cu), otherwise the query is searched again without an
 // estimate.  Results never depend on E.
-struct EstimatePlan {
-  bool on = false;
-  int rows = 0;    // sample rows (a multiple of 256)
-  int step = 1;    // sample row j is database row j * step
-  int blocks = 0;  // B = rows / 128 block minima per query
-  int j = 0;       // rank of the estimate among the block minima
-  FusedPlan plan;
-};
 
 // P(X >= j) for X ~ Binomial(n, q).
 double binomial_tail(int n, double q, int j) {
@@ -365,6 +358,9 @@ constexpr double kEstimateMuMin = 8.0;
 constexpr double kEstimateFailure = 1e-6;   // per-query failure probability for a uniform sample
 constexpr int kEstimateBlockRows = kHalfN;  // rows per block minimum (one epilogue warp's half tile)
 
+}  // namespace
+
+namespace curplsh_b200 {
 // The plan a search of this shape uses when the estimate is enabled (the
 // caller reads the process-wide switch once per search).
 EstimatePlan plan_estimate(int nq, long long n, int kp, int num_sms) {
@@ -387,6 +383,10 @@ EstimatePlan plan_estimate(int nq, long long n, int kp, int num_sms) {
   e.on = true;
   return e;
 }
+bool bound_estimate_enabled() { return g_bound_estimate.load(std::memory_order_relaxed) != 0; }
+}  // namespace curplsh_b200
+
+namespace {
 
 // Sizes and carve of one search's device workspace (search_device and
 // search_workspace_bytes use the same layout).
@@ -425,7 +425,7 @@ struct SearchBufs {
   float *qn = nullptr, *qs = nullptr;
   uint32_t* qbound = nullptr;   // [nq_pad] bounds of the full pass
   float* minima = nullptr;      // [nq_pad][B] block minima of the sample pass
-  int* fail = nullptr;          // [1 + nq]: count, then query indices
+  int* fail = nullptr;          // [2 + nq]: count, coarse-check count, then query indices
   int* counts = nullptr;
   uint64_t* pools = nullptr;
 };
@@ -438,7 +438,7 @@ size_t carve_search(Carve& c, const curplsh_index* ix, const SearchShape& sh, in
   b->qs = c.take<float>(sh.nq_pad);
   b->qbound = c.take<uint32_t>(sh.nq_pad);
   if (sh.est.on) b->minima = c.take<float>((size_t)sh.nq_pad * sh.est.blocks);
-  if (sh.est.on || sh.coarse) b->fail = c.take<int>(1 + (size_t)nq);
+  if (sh.est.on || sh.coarse) b->fail = c.take<int>(2 + (size_t)nq);
   b->counts = c.take<int>(sh.pool_lists);
   b->pools = c.take<uint64_t>(sh.pool_lists * (size_t)sh.P);
   return (size_t)round_up((long long)c.off, 256);
@@ -558,7 +558,7 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
   } else {
     CUDA_TRY(cudaMemsetAsync(b.qbound, 0xFF, (size_t)nq_pad * sizeof(uint32_t), st));
   }
-  if (b.fail) CUDA_TRY(cudaMemsetAsync(b.fail, 0, sizeof(int), st));
+  if (b.fail) CUDA_TRY(cudaMemsetAsync(b.fail, 0, 2 * sizeof(int), st));
   tm->rec(2, st);
 #ifdef CURPLSH_FUSED_STATS
   CUDA_TRY(fused_stats_begin(&f, st));
@@ -582,7 +582,8 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
   m.checks = (sh.est.on ? kCheckEstimate : 0) | (sh.coarse ? kCheckCoarse : 0);
   if (m.checks) {
     m.fail_count = b.fail;
-    m.fail_list = b.fail + 1;
+    m.coarse_count = b.fail + 1;
+    m.fail_list = b.fail + 2;
   }
   m.queries = q_dev;
   m.db = ix->x32;
@@ -609,7 +610,7 @@ size_t search_workspace_bytes(const curplsh_index* ix, int nq, int k, int form, 
   return carve_search(c, ix, sh, nq, form, &b) + 256;
 }
 
-// Searches again the `nf` queries listed at fail_dev + 1 (device) -- in the
+// Searches again the `nf` queries listed at fail_dev + 2 (device) -- in the
 // exact form, without an estimate, so no check applies -- and writes their
 // results into the full result arrays.
 int search_failed(curplsh_index* ix, int nf, const int* fail_dev, const float* q_dev, int k, int rerank_factor,
@@ -629,14 +630,13 @@ int search_failed(curplsh_index* ix, int nf, const int* fail_dev, const float* q
   float* qf = reinterpret_cast<float*>(base);
   int* oif = reinterpret_cast<int*>(base + qbytes);
   float* odf = reinterpret_cast<float*>(base + qbytes + (size_t)nf * k * sizeof(int));
-  CUDA_TRY(launch_gather_rows(q_dev, d, fail_dev + 1, nf, qf, st));
+  CUDA_TRY(launch_gather_rows(q_dev, d, fail_dev + 2, nf, qf, st));
   Timing none;
   int* again = nullptr;
   int rc = search_device(ix, nf, qf, k, form, rerank_factor, oif, odf, st, base + qbytes + obytes, &none, false,
                          false, &again);
   if (rc) return rc;
-  CUDA_TRY(launch_scatter_results(oif, odf, fail_dev + 1, nf, k, out_idx, out_dist, st));
-  ix->fallback_queries.fetch_add(nf, std::memory_order_relaxed);
+  CUDA_TRY(launch_scatter_results(oif, odf, fail_dev + 2, nf, k, out_idx, out_dist, st));
   return CURPLSH_OK;
 }
 
@@ -727,13 +727,15 @@ int do_search(curplsh_index* ix, int64_t num, const float* queries, int k, int p
   if (pass_ms) tm.rec(4, st);  // whole-search end (after copies)
   if (sync) {
     uint32_t* hw = static_cast<uint32_t*>(w.host.ptr);
-    hw[1] = 0;
+    hw[1] = hw[2] = 0;
     CUDA_TRY(cudaMemcpyAsync(hw, ix->status, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    if (fail) CUDA_TRY(cudaMemcpyAsync(hw + 1, fail, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (fail) CUDA_TRY(cudaMemcpyAsync(hw + 1, fail, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     uint32_t s = hw[0];
-    const int nf = (int)hw[1];
+    const int nf = (int)hw[1], nc = (int)hw[2];
     if (!s && nf > 0) {
+      ix->fallback_queries.fetch_add(nf - nc, std::memory_order_relaxed);
+      ix->coarse_queries.fetch_add(nc, std::memory_order_relaxed);
       // queries whose estimated bound was too small, or whose coarse margin
       // failed: search them again in the exact form
       rc = search_failed(ix, nf, fail, qd, k, rf, oi, od, st, w);
@@ -1159,6 +1161,12 @@ int curplsh_estimate_plan_shape(int64_t num_rows, int64_t num_queries, int kprim
 int curplsh_index_get_fallback_count(curplsh_index* ix, int64_t* count) {
   if (!ix || !count) return set_error(CURPLSH_ERR_INVALID_ARG, "null argument");
   *count = ix->fallback_queries.load(std::memory_order_relaxed);
+  return CURPLSH_OK;
+}
+
+int curplsh_index_get_coarse_fallback_count(curplsh_index* ix, int64_t* count) {
+  if (!ix || !count) return set_error(CURPLSH_ERR_INVALID_ARG, "null argument");
+  *count = ix->coarse_queries.load(std::memory_order_relaxed);
   return CURPLSH_OK;
 }
 

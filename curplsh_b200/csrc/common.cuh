@@ -120,6 +120,7 @@ struct FusedBatch {
   long long work_per_cta;  // W
   uint32_t* status;        // device error word
   unsigned long long* stats;  // per-role cycle counters, written only by builds with CURPLSH_FUSED_STATS
+  const int* run_if;       // non-null: every CTA returns at once unless *run_if != 0
 };
 
 // Counter slots of FusedBatch::stats (instrumented builds).

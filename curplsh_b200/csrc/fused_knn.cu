@@ -291,6 +291,10 @@ template <int FORM, int MAXI, bool MINIMA = false>
 __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_constant__ FusedArgs<MAXI> A) {
   using Tr = FormTraits<FORM>;
   const FusedBatch& B = A.B;
+  // a conditional pass (a re-search after a failed check): every thread of
+  // every CTA reads the same flag, written by an earlier launch on the stream,
+  // and leaves before any barrier or TMEM allocation when it is zero
+  if (B.run_if && *B.run_if == 0) return;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const SmemLayout L = make_layout(FORM, B.d);
@@ -948,7 +952,8 @@ cudaError_t ensure_attributes() {
 
 template <int FORM, int MAXI, bool MINIMA = false>
 cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, int n, const FusedBatchPlan& bp,
-                        uint32_t* status, unsigned long long* stats, uint32_t smem, cudaStream_t st) {
+                        uint32_t* status, unsigned long long* stats, uint32_t smem, cudaStream_t st,
+                        const int* run_if) {
   cudaError_t e = ensure_attributes<FORM, MAXI, MINIMA>();
   if (e != cudaSuccess) return e;
   FusedArgs<MAXI> a;
@@ -960,6 +965,7 @@ cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, 
   a.B.work_per_cta = bp.work_per_cta;
   a.B.status = status;
   a.B.stats = stats;
+  a.B.run_if = run_if;
   const bool fp8 = FORM == kFormFP8;
   for (int i = 0; i < n; ++i) {
     const FusedItemSpec& f = specs[i];
@@ -1015,12 +1021,14 @@ cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, 
 
 template <int FORM>
 cudaError_t launch_form_any(const FusedItemSpec* specs, const FusedItemPlan* plans, int n, const FusedBatchPlan& bp,
-                            uint32_t* status, unsigned long long* stats, uint32_t smem, cudaStream_t st) {
-  if (n == 1 && specs[0].minima) return launch_form<FORM, 1, true>(specs, plans, n, bp, status, stats, smem, st);
+                            uint32_t* status, unsigned long long* stats, uint32_t smem, cudaStream_t st,
+                            const int* run_if) {
+  if (n == 1 && specs[0].minima)
+    return launch_form<FORM, 1, true>(specs, plans, n, bp, status, stats, smem, st, run_if);
   for (int i = 0; i < n; ++i)
     if (specs[i].minima) return cudaErrorInvalidValue;  // block-minimum mode is single-item
-  if (n == 1) return launch_form<FORM, 1>(specs, plans, n, bp, status, stats, smem, st);
-  return launch_form<FORM, kFusedMaxItems>(specs, plans, n, bp, status, stats, smem, st);
+  if (n == 1) return launch_form<FORM, 1>(specs, plans, n, bp, status, stats, smem, st, run_if);
+  return launch_form<FORM, kFusedMaxItems>(specs, plans, n, bp, status, stats, smem, st, run_if);
 }
 
 }  // namespace
@@ -1095,7 +1103,7 @@ cudaError_t prepare_fused_kernels(int form) {
 
 cudaError_t launch_fused_batch(int form, const FusedItemSpec* specs, const FusedItemPlan* plans, int n,
                                const FusedBatchPlan& bp, uint32_t* status, unsigned long long* stats,
-                               cudaStream_t st) {
+                               cudaStream_t st, const int* run_if) {
   if (n < 1 || n > kFusedMaxItems) return cudaErrorInvalidValue;
   for (int i = 1; i < n; ++i)
     if (specs[i].d != specs[0].d) return cudaErrorInvalidValue;
@@ -1104,11 +1112,11 @@ cudaError_t launch_fused_batch(int form, const FusedItemSpec* specs, const Fused
   if (smem > 227u * 1024u) return cudaErrorInvalidConfiguration;  // a layout bug, not a caller error
   switch (form) {
     case kFormExact:
-      return launch_form_any<kFormExact>(specs, plans, n, bp, status, stats, smem, st);
+      return launch_form_any<kFormExact>(specs, plans, n, bp, status, stats, smem, st, run_if);
     case kFormBF16:
-      return launch_form_any<kFormBF16>(specs, plans, n, bp, status, stats, smem, st);
+      return launch_form_any<kFormBF16>(specs, plans, n, bp, status, stats, smem, st, run_if);
     case kFormFP8:
-      return launch_form_any<kFormFP8>(specs, plans, n, bp, status, stats, smem, st);
+      return launch_form_any<kFormFP8>(specs, plans, n, bp, status, stats, smem, st, run_if);
     default:
       return cudaErrorInvalidValue;
   }
@@ -1151,7 +1159,7 @@ cudaError_t launch_fused(const FusedLaunch& f, cudaStream_t st) {
   bp.total_work = ip.work_end;
   bp.work_per_cta = f.plan.work_per_cta;
   bp.grid = f.plan.grid;
-  return launch_fused_batch(f.form, &s, &ip, 1, bp, f.status, f.stats, st);
+  return launch_fused_batch(f.form, &s, &ip, 1, bp, f.status, f.stats, st, f.run_if);
 }
 
 }  // namespace curplsh_b200

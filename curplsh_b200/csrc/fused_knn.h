@@ -63,6 +63,7 @@ struct FusedLaunch {
   uint32_t* q_bound;
   uint32_t* status;
   unsigned long long* stats = nullptr;  // instrumented builds only
+  const int* run_if = nullptr;          // non-null: the launch does nothing unless *run_if != 0
   FusedPlan plan;
 };
 
@@ -115,9 +116,29 @@ void plan_fused_batch(const FusedItemSpec* specs, int n, int max_ctas, FusedItem
 // Sets the kernels' launch attributes on the current device (done lazily by
 // the launches; call it before a stream capture).
 cudaError_t prepare_fused_kernels(int form);
+// `run_if` (optional, device): every CTA returns at once unless *run_if != 0
+// (a pass that must run only after a failed check, decided on the device).
 cudaError_t launch_fused_batch(int form, const FusedItemSpec* specs, const FusedItemPlan* plans, int n,
                                const FusedBatchPlan& bp, uint32_t* status, unsigned long long* stats,
-                               cudaStream_t st);
+                               cudaStream_t st, const int* run_if = nullptr);
+
+// ---- sampled bound estimate (capi.cpp): a short fused pass over a strided
+// sample of the database records per query the smallest distance of every
+// 128-row block of the sample; the j-th smallest of those B block minima is
+// the starting bound of every candidate pool of the full pass.
+struct EstimatePlan {
+  bool on = false;
+  int rows = 0;    // sample rows (a multiple of 256)
+  int step = 1;    // sample row j is database row j * step
+  int blocks = 0;  // B = rows / 128 block minima per query
+  int j = 0;       // rank of the estimate among the block minima
+  FusedPlan plan;
+};
+// The estimate a search of nq queries with k' candidates against n rows uses
+// (on == false: none), whatever the process-wide switch says.
+EstimatePlan plan_estimate(int nq, long long n, int kp, int num_sms);
+// The process-wide switch (curplsh_set_bound_estimate).
+bool bound_estimate_enabled();
 
 // Row preparation: squared norms (FP32), BF16 hi/lo split, FP8-E4M3 with a
 // per-row FP32 scale.  Rows in [nrows, nrows_pad) are written as zeros with
@@ -161,6 +182,7 @@ constexpr int kCheckCoarse = 2;    // coarse (BF16/FP8) distances: verify the ca
 struct MergeLaunch {
   int nq, nb, d, k, kprime, pool_cap;
   int checks = 0;                // kCheck* bits; any bit needs fail_count / fail_list
+  int* coarse_count = nullptr;   // kCheckCoarse: queries listed by that check (may be null)
   FusedPlan plan;
   const uint64_t* pools;
   const int* pool_counts;
@@ -204,6 +226,7 @@ struct MergeItem {
   long long nb_total;      // database rows (kCheckCoarse: nothing to check when k' covers them all)
   int* fail_count;
   int* fail_list;
+  int* coarse_count;       // kCheckCoarse: counts the queries that check listed (may be null)
   const float* queries;    // [nq x d] fp32, row stride d
   const float* db;         // database rows fp32, row stride ld_db
   long long ld_db;
@@ -212,11 +235,14 @@ struct MergeItem {
   int* out_idx;            // [nq x k]
   float* out_dist;
 };
-cudaError_t launch_merge_batch(MergeItem* items, int n, int d, uint32_t* status, cudaStream_t st);
+cudaError_t launch_merge_batch(MergeItem* items, int n, int d, uint32_t* status, cudaStream_t st,
+                               const int* run_if = nullptr);
 cudaError_t prepare_merge_kernel();
 
 // Fill [n] ints / floats (N == 0 results, padding).
 cudaError_t launch_fill_results(int* idx, float* dist, long long n, cudaStream_t st);
+// p[i] = v for i < n, only when *cond != 0 (decided on the device).
+cudaError_t launch_fill_u32_if(uint32_t* p, long long n, uint32_t v, const int* cond, cudaStream_t st);
 // out[q] = order bits of the j-th smallest (1-based) of minima[q * count ..
 // q * count + count) for q < nq (all ones when count < j).
 cudaError_t launch_estimate_select(const float* minima, int count, int nq, int j, uint32_t* out, cudaStream_t st);

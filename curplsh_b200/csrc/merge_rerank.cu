@@ -51,6 +51,7 @@ struct MergeArgs {
   int lcnt_n;   // room for the largest list count, rounded to 4
   int vec4;     // query and database rows allow 16-byte loads
   uint32_t* status;
+  const int* run_if;  // non-null: the launch does nothing unless *run_if != 0
 };
 
 // Block-wide radix select: the bound B such that exactly `keep` of the keys
@@ -90,6 +91,7 @@ __device__ uint64_t block_select_bound(Each each, uint32_t keep, uint32_t* hist,
 }
 
 __global__ void __launch_bounds__(kMergeThreads) merge_rerank_kernel(const __grid_constant__ MergeArgs a) {
+  if (a.run_if && *a.run_if == 0) return;  // a conditional re-merge whose check passed
   int lo = 0, hi = a.num_items - 1;  // last item with q_begin <= blockIdx.x
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
@@ -334,6 +336,7 @@ __global__ void __launch_bounds__(kMergeThreads) merge_rerank_kernel(const __gri
     if (!(cmax - dk >= emax + (emax - emin))) {
       const int pos = atomicAdd(m.fail_count, 1);
       m.fail_list[pos] = q;
+      if (m.coarse_count) atomicAdd(m.coarse_count, 1);
     }
   }
   for (int t = tid; t < m.k; t += kMergeThreads) {
@@ -364,7 +367,8 @@ cudaError_t prepare_merge_kernel() {
   return cudaSuccess;
 }
 
-cudaError_t launch_merge_batch(MergeItem* items, int n, int d, uint32_t* status, cudaStream_t st) {
+cudaError_t launch_merge_batch(MergeItem* items, int n, int d, uint32_t* status, cudaStream_t st,
+                               const int* run_if) {
   if (n < 1 || n > kMergeMaxItems) return cudaErrorInvalidValue;
   MergeArgs a;
   memset(&a, 0, sizeof(a));
@@ -381,6 +385,7 @@ cudaError_t launch_merge_batch(MergeItem* items, int n, int d, uint32_t* status,
   a.num_items = n;
   a.d = d;
   a.status = status;
+  a.run_if = run_if;
   int kp2 = 32;  // >= 32 keeps the shared-memory carve 16-byte aligned
   while (kp2 < kpmax) kp2 <<= 1;
   a.kp2 = kp2;
@@ -429,6 +434,7 @@ cudaError_t launch_merge_rerank(const MergeLaunch& m, cudaStream_t st) {
   it.checks = m.checks;
   it.nb_total = m.nb;
   it.fail_count = m.fail_count;
+  it.coarse_count = m.coarse_count;
   it.fail_list = m.fail_list;
   it.queries = m.queries;
   it.db = m.db;

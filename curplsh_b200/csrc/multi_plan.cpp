@@ -42,6 +42,7 @@ int MultiPlan::build(const curplsh_batch_item* items, int n, const std::vector<c
   groups_.clear();
   base_ = nullptr;
   status_ = nullptr;
+  const bool use_est = bound_estimate_enabled();  // read once: planning and enqueue agree
 
   // ---- fused items: (index, form, k') -> concatenated queries
   std::map<std::tuple<int, int, int>, int> fmap;
@@ -141,6 +142,9 @@ int MultiPlan::build(const curplsh_batch_item* items, int n, const std::vector<c
         FItem& x = fitems_[FL.fitems[j]];
         x.plan = plans[j];
         x.W = FL.bp.work_per_cta;
+        x.launch = (int)(&FL - G.launches.data());
+        if (use_est) x.est = plan_estimate(x.nq, views[x.slot].n, x.kp, num_sms);
+        FL.est_any = FL.est_any || x.est.on;
       }
     }
   }
@@ -156,6 +160,22 @@ int MultiPlan::build(const curplsh_batch_item* items, int n, const std::vector<c
   bounds_words_ = 0;
   for (const FItem& x : fitems_) bounds_words_ += (size_t)x.nq_pad;
   o_bounds_ = take(bounds_words_ * sizeof(uint32_t));
+  // failure lists of the launches that verify an estimate, in one region
+  // (cleared by one memset per run)
+  size_t fail_ints = 0;
+  for (Group& G : groups_)
+    for (FLaunch& FL : G.launches) {
+      if (!FL.est_any) continue;
+      FL.o_fail = fail_ints * sizeof(int);
+      fail_ints += 2;
+      for (int fi : FL.fitems) fail_ints += (size_t)fitems_[fi].nq;
+      fail_ints = (size_t)rup((long long)fail_ints, 64);
+    }
+  fails_bytes_ = fail_ints * sizeof(int);
+  o_fails_ = take(fails_bytes_);
+  for (Group& G : groups_)
+    for (FLaunch& FL : G.launches)
+      if (FL.est_any) FL.o_fail += o_fails_;
   size_t bcur = 0;
   for (FItem& x : fitems_) {
     const IndexView& v = views[x.slot];
@@ -170,6 +190,7 @@ int MultiPlan::build(const curplsh_batch_item* items, int n, const std::vector<c
     x.o_qs = take((size_t)x.nq_pad * 4);
     x.o_counts = take(lists * 4);
     x.o_pools = take(lists * (size_t)x.P * 8);
+    if (x.est.on) x.o_minima = take((size_t)x.nq_pad * x.est.blocks * sizeof(float));
   }
   bytes_ = (size_t)rup((long long)off, 256) + 256;
   views_ = views;
@@ -215,6 +236,7 @@ int MultiPlan::enqueue(cudaStream_t main, const std::vector<cudaStream_t>* branc
   int kernels = 0;
   MP_TRY(cudaMemsetAsync(status_, 0, sizeof(uint32_t), main));
   if (bounds_words_) MP_TRY(cudaMemsetAsync(base_ + o_bounds_, 0xFF, bounds_words_ * sizeof(uint32_t), main));
+  if (fails_bytes_) MP_TRY(cudaMemsetAsync(base_ + o_fails_, 0, fails_bytes_, main));
   const bool fan = branches && joins && fork && groups_.size() > 1;
   if (fan) MP_TRY(cudaEventRecord(fork, main));
   for (size_t gi = 0; gi < groups_.size(); ++gi) {
@@ -265,61 +287,139 @@ int MultiPlan::enqueue(cudaStream_t main, const std::vector<cudaStream_t>* branc
     }
     int rc = flush_prep();
     if (rc) return rc;
+    // sampled bound estimates: the block-minimum pass over the sample and the
+    // rank select, which overwrites the item's all-ones bounds
+    for (int fi : G.fitems) {
+      const FItem& x = fitems_[fi];
+      if (!x.est.on) continue;
+      const FusedItemSpec& s = x.spec;
+      FusedLaunch e{};
+      e.nq = s.nq;
+      e.nb = x.est.rows;
+      e.d = s.d;
+      e.kprime = 1;
+      e.pool_cap = s.pool_cap;
+      e.form = G.form;
+      e.nq_pad = s.nq_pad;
+      e.nb_pad = x.est.rows;
+      e.ld16 = s.ld16;
+      e.ld8 = s.ld8;
+      e.qh = s.qh;
+      e.ql = s.ql;
+      e.q8 = s.q8;
+      e.qn = s.qn;
+      e.qs = s.qs;
+      e.xh = s.xh;
+      e.xl = s.xl;
+      e.x8 = s.x8;
+      e.xn = s.xn;
+      e.xs = s.xs;
+      e.db_step = x.est.step;
+      e.minima = reinterpret_cast<float*>(base_ + x.o_minima);
+      e.pools = s.pools;
+      e.pool_counts = s.pool_counts;
+      e.q_bound = s.q_bound;
+      e.status = status_;
+      e.plan = x.est.plan;
+      MP_TRY(launch_fused(e, st));
+      MP_TRY(launch_estimate_select(e.minima, x.est.blocks, x.nq, x.est.j, s.q_bound, st));
+      kernels += 2;
+    }
     // fused filter
-    for (const FLaunch& FL : G.launches) {
+    auto fused_launch = [&](const FLaunch& FL, const int* run_if) -> int {
       std::vector<FusedItemSpec> specs;
       std::vector<FusedItemPlan> plans;
       for (int fi : FL.fitems) {
         specs.push_back(fitems_[fi].spec);
         plans.push_back(fitems_[fi].plan);
       }
-      MP_TRY(launch_fused_batch(G.form, specs.data(), plans.data(), (int)specs.size(), FL.bp, status_, nullptr, st));
+      MP_TRY(launch_fused_batch(G.form, specs.data(), plans.data(), (int)specs.size(), FL.bp, status_, nullptr, st,
+                                run_if));
       if (FL.bp.grid > 0) ++kernels;
+      return CURPLSH_OK;
+    };
+    for (const FLaunch& FL : G.launches) {
+      rc = fused_launch(FL, nullptr);
+      if (rc) return rc;
     }
     // merge + exact rerank: one item per member; one launch per power-of-two
     // class of k' so that small-k requests do not reserve the shared memory
-    // of the largest k'
-    std::map<int, std::vector<MergeItem>> by_class;
-    for (int fi : G.fitems) {
-      const FItem& x = fitems_[fi];
-      const IndexView& v = views_[x.slot];
-      int cls = 32;
-      while (cls < x.kp) cls <<= 1;
-      for (size_t j = 0; j < x.members.size(); ++j) {
-        const curplsh_batch_item& it = items_[x.members[j]];
-        MergeItem m{};
-        m.nq = (int)it.num;
-        m.k = it.k;
-        m.kprime = x.kp;
-        m.pool_cap = x.P;
-        m.num_tiles = v.n > 0 ? x.plan.num_tiles : 0;
-        m.units_per_block = v.n > 0 ? x.plan.units_per_block : 1;
-        m.row0 = x.row0[j];
-        m.split_tiles = v.n > 0 ? x.plan.split_tiles : 1;
-        m.work_begin = x.plan.work_begin;
-        m.work_per_cta = x.W;
-        m.pools = x.spec.pools;
-        m.pool_counts = x.spec.pool_counts;
-        m.q_bound = x.spec.q_bound;
-        m.fail_count = nullptr;
-        m.fail_list = nullptr;
-        m.queries = it.queries;
-        m.db = v.x32;
-        m.ld_db = v.dim;
-        m.db16 = v.bf16_exact ? v.xh : nullptr;
-        m.ld16 = v.ld16;
-        m.out_idx = it.indices;
-        m.out_dist = it.distances;
-        by_class[cls].push_back(m);
+    // of the largest k'.  `only` (>= 0) restricts it to the items of one fused
+    // launch, the fallback's merges after a failed estimate (no checks, run
+    // only when the launch's failure count is nonzero).
+    auto merge_items = [&](int only, std::map<int, std::vector<MergeItem>>& by_class) {
+      for (int fi : G.fitems) {
+        const FItem& x = fitems_[fi];
+        const IndexView& v = views_[x.slot];
+        if (only >= 0 && x.launch != only) continue;
+        int* fcnt = (x.est.on && only < 0) ? reinterpret_cast<int*>(base_ + G.launches[x.launch].o_fail) : nullptr;
+        int cls = 32;
+        while (cls < x.kp) cls <<= 1;
+        for (size_t j = 0; j < x.members.size(); ++j) {
+          const curplsh_batch_item& it = items_[x.members[j]];
+          MergeItem m{};
+          m.nq = (int)it.num;
+          m.k = it.k;
+          m.kprime = x.kp;
+          m.pool_cap = x.P;
+          m.num_tiles = v.n > 0 ? x.plan.num_tiles : 0;
+          m.units_per_block = v.n > 0 ? x.plan.units_per_block : 1;
+          m.row0 = x.row0[j];
+          m.split_tiles = v.n > 0 ? x.plan.split_tiles : 1;
+          m.work_begin = x.plan.work_begin;
+          m.work_per_cta = x.W;
+          m.pools = x.spec.pools;
+          m.pool_counts = x.spec.pool_counts;
+          m.q_bound = x.spec.q_bound;
+          m.checks = fcnt ? kCheckEstimate : 0;
+          m.nb_total = v.n;
+          m.fail_count = fcnt;
+          m.fail_list = fcnt ? fcnt + 2 : nullptr;
+          m.coarse_count = nullptr;
+          m.queries = it.queries;
+          m.db = v.x32;
+          m.ld_db = v.dim;
+          m.db16 = v.bf16_exact ? v.xh : nullptr;
+          m.ld16 = v.ld16;
+          m.out_idx = it.indices;
+          m.out_dist = it.distances;
+          by_class[cls].push_back(m);
+        }
       }
+    };
+    auto merge_launches = [&](std::map<int, std::vector<MergeItem>>& by_class, const int* run_if) -> int {
+      for (auto& kv : by_class) {
+        std::vector<MergeItem>& all = kv.second;
+        for (size_t s0 = 0; s0 < all.size(); s0 += kMergeMaxItems) {
+          const int cnt = (int)std::min<size_t>(kMergeMaxItems, all.size() - s0);
+          MP_TRY(launch_merge_batch(all.data() + s0, cnt, G.d, status_, st, run_if));
+          ++kernels;
+        }
+      }
+      return CURPLSH_OK;
+    };
+    {
+      std::map<int, std::vector<MergeItem>> by_class;
+      merge_items(-1, by_class);
+      rc = merge_launches(by_class, nullptr);
+      if (rc) return rc;
     }
-    for (auto& kv : by_class) {
-      std::vector<MergeItem>& all = kv.second;
-      for (size_t s0 = 0; s0 < all.size(); s0 += kMergeMaxItems) {
-        const int cnt = (int)std::min<size_t>(kMergeMaxItems, all.size() - s0);
-        MP_TRY(launch_merge_batch(all.data() + s0, cnt, G.d, status_, st));
+    // fallback chains: a launch with a failed estimate runs again without it
+    for (size_t li = 0; li < G.launches.size(); ++li) {
+      const FLaunch& FL = G.launches[li];
+      if (!FL.est_any) continue;
+      const int* fcnt = reinterpret_cast<const int*>(base_ + FL.o_fail);
+      for (int fi : FL.fitems) {
+        const FItem& x = fitems_[fi];
+        MP_TRY(launch_fill_u32_if(x.spec.q_bound, x.nq_pad, 0xFFFFFFFFu, fcnt, st));
         ++kernels;
       }
+      rc = fused_launch(FL, fcnt);
+      if (rc) return rc;
+      std::map<int, std::vector<MergeItem>> by_class;
+      merge_items((int)li, by_class);
+      rc = merge_launches(by_class, fcnt);
+      if (rc) return rc;
     }
     if (fan) {
       MP_TRY(cudaEventRecord((*joins)[gi], st));

@@ -10,7 +10,14 @@
 //     concatenated into one fused item whose queries share 128-row blocks;
 //   * fused items are grouped by (form, d): per group one segmented prep
 //     launch, persistent fused launches of up to kFusedMaxItems items, and one
-//     merge + rerank launch per power-of-two class of k'.
+//     merge + rerank launch per power-of-two class of k';
+//   * a fused item large enough for the sampled bound estimate starts its
+//     pools from it, exactly as a single search does; the merge verifies the
+//     estimate on the device, and when any query of a fused launch failed,
+//     a fallback chain enqueued behind it (bounds reset, the fused launch and
+//     its merges again, without the estimate) runs -- every kernel of it reads
+//     the launch's failure count first and does nothing when it is zero, so
+//     the plan needs no host round trip and can be captured in a graph.
 // build() sizes everything without allocating; bind() places the working
 // memory in a caller-provided range; enqueue() issues the launches.
 #pragma once
@@ -58,11 +65,16 @@ class MultiPlan {
     FusedItemSpec spec{};
     FusedItemPlan plan{};
     long long W = 1;
+    EstimatePlan est;   // est.on: the full pass starts from the sampled bound estimate
+    int launch = -1;    // index of its fused launch within its group
     size_t o_qh = 0, o_ql = 0, o_q8 = 0, o_qn = 0, o_qs = 0, o_counts = 0, o_pools = 0, o_bounds = 0;
+    size_t o_minima = 0;
   };
   struct FLaunch {
     std::vector<int> fitems;
     FusedBatchPlan bp;
+    bool est_any = false;  // some item uses the estimate: verification and the fallback chain
+    size_t o_fail = 0;     // [2 + queries]: failure count, (unused), failed query indices
   };
   struct Group {
     int form = 0, d = 0;
@@ -74,7 +86,7 @@ class MultiPlan {
   std::vector<IndexView> views_;
   std::vector<FItem> fitems_;
   std::vector<Group> groups_;
-  size_t bytes_ = 0, o_status_ = 0, o_bounds_ = 0, bounds_words_ = 0;
+  size_t bytes_ = 0, o_status_ = 0, o_bounds_ = 0, bounds_words_ = 0, o_fails_ = 0, fails_bytes_ = 0;
   char* base_ = nullptr;
   uint32_t* status_ = nullptr;
 };

@@ -240,6 +240,12 @@ __global__ void fill_results_kernel(int* idx, float* dist, long long n) {
   }
 }
 
+__global__ void fill_u32_if_kernel(uint32_t* p, long long n, uint32_t v, const int* cond) {
+  if (*cond == 0) return;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
 // One warp per query: the j-th smallest (1-based) of `count` floats, by a
 // most-significant-digit radix select on their order bits (4 passes of 8
 // bits, a 256-bin warp histogram in shared memory).
@@ -367,6 +373,14 @@ cudaError_t launch_l2_norms(const float* x, long long n, int d, float* norms, in
   const int vec4 = (d % 4 == 0) && ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
   const long long blocks = (n + kPrepWarps - 1) / kPrepWarps;
   l2_norms_kernel<<<(unsigned)blocks, kPrepWarps * 32, 0, st>>>(x, n, d, norms, squared, vec4);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill_u32_if(uint32_t* p, long long n, uint32_t v, const int* cond, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  long long blocks = (n + 255) / 256;
+  if (blocks > 1024) blocks = 1024;
+  fill_u32_if_kernel<<<(unsigned)blocks, 256, 0, st>>>(p, n, v, cond);
   return cudaGetLastError();
 }
 

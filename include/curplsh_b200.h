@@ -301,8 +301,7 @@ int curplsh_index_estimate_plan(curplsh_index* index, int64_t num_queries, int k
  * on. */
 int curplsh_estimate_plan_shape(int64_t num_rows, int64_t num_queries, int kprime, int num_sms, int* sample_rows,
                                 int* step, int* rank);
-/* Number of queries this index searched again (since creation) because their estimate or their
- * coarse margin (below) failed. */
+/* Number of queries this index searched again after their estimate failed (since creation). */
 int curplsh_index_get_fallback_count(curplsh_index* index, int64_t* count);
 
 /* ------------------------------------------------------------ coarse-margin check */
@@ -313,12 +312,15 @@ int curplsh_index_get_fallback_count(curplsh_index* index, int64_t* count);
  * of the candidates themselves: when the margin is smaller than the largest error plus the
  * errors' spread, the coarse form is too coarse for this query's data and the query is searched
  * again in the FP32-exact form before the call returns (counted by
- * curplsh_index_get_fallback_count).  Forms whose coarse distances are exact for the data (BF16
+ * curplsh_index_get_coarse_fallback_count).  Forms whose coarse distances are exact for the data (BF16
  * on integer or BF16-valued rows) always pass.  It is a check of the data against the form's
  * precision, not a proof.  Applies to curplsh_index_search / _ex / _profiled; a search that uses
  * it returns synchronised even with device buffers.  Process-wide; on (1) by default. */
 int curplsh_set_coarse_check(int enabled);
 int curplsh_get_coarse_check(int* enabled);
+/* Number of queries this index searched again in the exact form after their coarse margin
+ * failed (since creation). */
+int curplsh_index_get_coarse_fallback_count(curplsh_index* index, int64_t* count);
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -39,7 +39,7 @@ def _search(cb, res, base, queries, k, form):
     ix = cb.IndexBF(res, base.shape[1], cb.IndexBFConfig(precision=form))
     ix.add(base.shape[0], base)
     d, i = ix.search_array(queries, k)
-    fb = ix.fallback_count()
+    fb = ix.coarse_fallback_count()
     ix.close()
     return d, i, fb
 

@@ -22,8 +22,12 @@ def cb():
     import torch
     assert torch.cuda.is_available(), "GPU tests need a CUDA device"
     import curplsh_b200
+    # these tests compare paths that differ only in the estimate: the coarse
+    # check (host searches only) stays off so that it cannot tell them apart
+    curplsh_b200.set_coarse_check(False)
     yield curplsh_b200
     curplsh_b200.set_bound_estimate(True)
+    curplsh_b200.set_coarse_check(True)
 
 
 @pytest.fixture(scope="module")
