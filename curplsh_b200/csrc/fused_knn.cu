@@ -264,6 +264,11 @@ __device__ __forceinline__ float thr_from(float dstar, float qn) {
 // A chunk of 64 columns whose passing lanes (minimum under the bound) number at
 // most this many is filtered lane by lane through the warp's staging buffer;
 // with more, every lane builds its survivor masks (a pool with no bound yet).
+// 1: an epilogue warp releases the accumulator as soon as its last TMEM read
+// of the tile has landed (before filtering that chunk); 0: after filtering.
+#ifndef CURPLSH_EARLY_RELEASE
+#define CURPLSH_EARLY_RELEASE 1
+#endif
 #ifndef CURPLSH_STAGED_LANES
 #define CURPLSH_STAGED_LANES 6
 #endif
@@ -635,6 +640,15 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
           tmem_ld_32x32b_x64(tmem_base + lane_base + slot * kBN + g * kHalfN + h * 64, v);
           tmem_ld_wait();
           STAT_END(ttm, st_tmem);
+#if CURPLSH_EARLY_RELEASE
+          if (h == kHalfN / 64 - 1) {
+            // this warp's last TMEM read of the tile has landed: hand the
+            // accumulator back to the MMA issuer before filtering the chunk
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[slot]);
+          }
+#endif
           const int col0 = colh + h * 64;
           // coarse distances of the 64 columns (two independent 32-column halves)
           float da[32], db[32];
@@ -836,9 +850,11 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
         if (MINIMA && valid)
           p.minima[(size_t)q * (2 * (size_t)p.num_tiles) + 2 * (size_t)tphys + g] =
               Tr::kFolded ? bmin : bmin + qn;
+#if !CURPLSH_EARLY_RELEASE
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(&acc_empty[slot]);
+#endif
         STAT_END(tfl, st_filter);
         }  // got
         // every S tiles (and at the unit's end) meet the partner warp; leave
