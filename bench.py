@@ -632,7 +632,11 @@ def run_serving(cb, synth, args, world, rank, local, res):
             sizes = request_sizes(count)
             gaps = rng.exponential(1.0 / mean_req, size=count)
             arrivals = np.cumsum(gaps) - gaps[0]
+            sampler = ClockSampler(local)
+            sampler.__enter__()
             lat, wall, (_, _, ph) = run_load(srv, sizes, list(arrivals))
+            sampler.__exit__(None, None, None)
+            sm = [float(x.split(",")[0]) for x in sampler.lines if x and x.split(",")[0].strip().replace(".", "").isdigit()]
             slow = np.argsort(-lat)[:3]
             ph = np.array(ph) * 1e3
             per_rate[str(rate)] = {"p50_ms": float(np.percentile(lat, 50) * 1e3),
@@ -643,7 +647,9 @@ def run_serving(cb, synth, args, world, rank, local, res):
                                                      "retire": float(np.percentile(ph[:, 2], 99))},
                                    "slowest": [[int(i), sizes[i], round(float(lat[i] * 1e3), 3),
                                                 [round(float(x), 3) for x in ph[i]]] for i in slow],
-                                   "achieved_queries_per_s": sum(sizes) / wall, "requests": count}
+                                   "achieved_queries_per_s": sum(sizes) / wall, "requests": count,
+                                   "sm_mhz": {"median": statistics.median(sm) if sm else None,
+                                              "min": min(sm) if sm else None, "samples": len(sm)}}
         st = srv.stats()
         srv.close()
         forms_out[FORMS[form]] = {"saturated_queries_per_s": sat, "rates": per_rate, **st}
@@ -721,6 +727,18 @@ def main():
         barrier(world)
         return rc
 
+    # the reference's own GPU path first, in subprocesses, before this process
+    # creates its CUDA context (two contexts on one GPU time-slice)
+    wanted = [c for c in args.configs.split(",") if c and c != "none"] if world == 1 else []
+    ref_gpu = None
+    if "reference_gpu" in wanted and args.workload in WORKLOADS:
+        t0 = time.perf_counter()
+        try:
+            ref_gpu = run_reference_gpu(args)
+        except Exception as e:  # noqa: BLE001
+            ref_gpu = {"error": f"{type(e).__name__}: {e}"[:400]}
+        ref_gpu["bench_s"] = time.perf_counter() - t0
+
     import torch
 
     import curplsh_b200 as cb
@@ -749,9 +767,12 @@ def main():
 
     head = run_single(cb, synth, args.workload, args, world, rank, local, res, peaks, fp8_peak, with_clocks=True)
     configs = {}
-    wanted = [c for c in args.configs.split(",") if c and c != "none"] if world == 1 else []
     for c in wanted:
         if c == args.workload:
+            continue
+        if c == "reference_gpu":
+            if ref_gpu is not None:
+                configs[c] = ref_gpu
             continue
         t0 = time.perf_counter()
         try:
@@ -761,8 +782,6 @@ def main():
                 r = run_batched(cb, synth, args, world, rank, local, res, peaks)
             elif c == "serving":
                 r = run_serving(cb, synth, args, world, rank, local, res)
-            elif c == "reference_gpu":
-                r = run_reference_gpu(args)
             else:
                 continue
         except Exception as e:  # noqa: BLE001  (a failed sub-record must not lose the headline)

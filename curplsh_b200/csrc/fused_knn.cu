@@ -92,7 +92,6 @@ struct SmemLayout {
   uint32_t bar_off;    // offset of the barrier block
   uint32_t hist_off;   // warp-private radix histograms
   uint32_t pool_off;   // per-row candidate pool counts and bounds
-  uint32_t stage_off;  // FP8: warp-private 64-float survivor staging (the folded forms use the histogram area)
   uint32_t total;      // dynamic smem bytes requested (includes 1 KB alignment slack)
 };
 
@@ -108,8 +107,7 @@ __host__ __device__ inline SmemLayout make_layout(int form, int d) {
   // the tail runs the hi x hi product alone, which is exact only for those
   L.tail_narrow = folded && (d % 64 == 0);
   // everything below the barrier block must fit the 227 KB opt-in limit
-  const uint32_t stage_buf = folded ? 0u : (uint32_t)kEpiWarps * 64u * 4u;
-  const uint32_t budget = 227u * 1024u - 256u - (uint32_t)kEpiWarps * 256u * 4u - 1024u - stage_buf - 1024u;
+  const uint32_t budget = 227u * 1024u - 256u - (uint32_t)kEpiWarps * 256u * 4u - 1024u - 1024u;
   const int nreg = L.nkc - (L.tail_narrow ? 1 : 0);
   const uint32_t a_res = (uint32_t)nreg * a_parts * kAChunkBytes + (L.tail_narrow ? kATailBytes : 0u);
   // a stage = one regular K chunk of the tile; the last one also carries the tail
@@ -129,8 +127,7 @@ __host__ __device__ inline SmemLayout make_layout(int form, int d) {
   L.bar_off = L.a_bytes + (uint32_t)L.stages * L.stage_bytes;
   L.hist_off = L.bar_off + 256;  // barriers: 2*8 + 6 mbarriers + tmem slot + flags < 256 B
   L.pool_off = L.hist_off + kEpiWarps * 256 * 4;
-  L.stage_off = L.pool_off + 1024;
-  L.total = L.stage_off + stage_buf + 1024;
+  L.total = L.pool_off + 1024 + 1024;
   return L;
 }
 
@@ -261,18 +258,11 @@ __device__ __forceinline__ float thr_from(float dstar, float qn) {
 #define STAT_FLUSH(slot, acc)
 #endif
 
-// A chunk of 64 columns whose passing lanes (minimum under the bound) number at
-// most this many is filtered lane by lane through the warp's staging buffer;
-// with more, every lane builds its survivor masks (a pool with no bound yet).
 // 1: an epilogue warp releases the accumulator as soon as its last TMEM read
 // of the tile has landed (before filtering that chunk); 0: after filtering.
 #ifndef CURPLSH_EARLY_RELEASE
-#define CURPLSH_EARLY_RELEASE 1
+#define CURPLSH_EARLY_RELEASE 0
 #endif
-#ifndef CURPLSH_STAGED_LANES
-#define CURPLSH_STAGED_LANES 6
-#endif
-constexpr int kStagedLanes = CURPLSH_STAGED_LANES;
 
 // v[j] for a runtime j in [0, 32) without local memory: a 5-level select tree.
 __device__ __forceinline__ float select32(const float (&v)[32], int j) {
@@ -696,78 +686,6 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
             bmin = fminf(bmin, mm[0]);
             continue;
           }
-          // Columns past nb (padding rows of the last tile) never survive.
-          const int lim = p.nb - col0;
-          if (lim < 64) {
-#pragma unroll
-            for (int j = 0; j < 32; ++j) {
-              if (j >= lim) da[j] = __uint_as_float(0x7F800000u);  // +inf
-              if (32 + j >= lim) db[j] = __uint_as_float(0x7F800000u);
-            }
-          }
-          // A lane's smallest coarse distance of the 64 columns decides whether
-          // it has any survivor: one three-input min per three columns, instead
-          // of a compare-and-mask step per column.  Most lanes have none.
-          float mn;
-          {
-            auto at = [&](int j) -> float { return j < 32 ? da[j] : db[j - 32]; };
-            float m1[22];
-#pragma unroll
-            for (int i = 0; i < 21; ++i) m1[i] = fmin3(at(3 * i), at(3 * i + 1), at(3 * i + 2));
-            m1[21] = at(63);
-            float m2[8];
-#pragma unroll
-            for (int i = 0; i < 7; ++i) m2[i] = fmin3(m1[3 * i], m1[3 * i + 1], m1[3 * i + 2]);
-            m2[7] = m1[21];
-            mn = fmin3(fmin3(m2[0], m2[1], m2[2]), fmin3(m2[3], m2[4], m2[5]), fminf(m2[6], m2[7]));
-          }
-          const uint32_t flagged = __ballot_sync(0xffffffffu, valid && mn <= thr);
-          if (flagged == 0u) continue;
-          STAT_INC(st_slow, 1);
-          if (__popc(flagged) <= kStagedLanes) {
-            // Few lanes pass: each in turn stages its 64 distances in the
-            // warp's buffer, the whole warp compares them with that lane's
-            // bound (two columns per thread) and appends the survivors to the
-            // lane's pool in parallel.
-            float* buf = Tr::kFolded ? reinterpret_cast<float*>(hist)
-                                     : reinterpret_cast<float*>(smem + L.stage_off) + ew * 64;
-            uint32_t rem = flagged;
-            while (rem) {
-              const int src = __ffs(rem) - 1;
-              rem &= rem - 1;
-              if (lane == src) {
-                float4* b4 = reinterpret_cast<float4*>(buf);
-#pragma unroll
-                for (int j4 = 0; j4 < 8; ++j4) {
-                  b4[j4] = make_float4(da[4 * j4], da[4 * j4 + 1], da[4 * j4 + 2], da[4 * j4 + 3]);
-                  b4[8 + j4] = make_float4(db[4 * j4], db[4 * j4 + 1], db[4 * j4 + 2], db[4 * j4 + 3]);
-                }
-              }
-              __syncwarp();
-              const float t_src = __shfl_sync(0xffffffffu, thr, src);
-              const float qn_src = Tr::kFolded ? 0.f : __shfl_sync(0xffffffffu, qn, src);
-              const float x0 = buf[lane], x1 = buf[32 + lane];
-              const bool s0 = x0 <= t_src, s1 = x1 <= t_src;  // padding columns hold values above any bound
-              const uint32_t b0 = __ballot_sync(0xffffffffu, s0), b1 = __ballot_sync(0xffffffffu, s1);
-              int base = 0;
-              if (lane == src) base = atomicAdd(&cnt_s[row], __popc(b0) + __popc(b1));
-              base = __shfl_sync(0xffffffffu, base, src);
-              uint64_t* pool_src = pool_of(lg * 32 + src);
-              const uint32_t below = (1u << lane) - 1u;
-              if (s0) {
-                const int pos = base + __popc(b0 & below);
-                if (pos < P) pool_src[pos] = make_key(Tr::kFolded ? x0 : x0 + qn_src, (uint32_t)(col0 + lane));
-              }
-              if (s1) {
-                const int pos = base + __popc(b0) + __popc(b1 & below);
-                if (pos < P)
-                  pool_src[pos] = make_key(Tr::kFolded ? x1 : x1 + qn_src, (uint32_t)(col0 + 32 + lane));
-              }
-              STAT_INC(st_surv, lane == src ? __popc(b0) + __popc(b1) : 0);
-              __syncwarp();  // the buffer is refilled by the next lane
-            }
-            continue;
-          }
           // survivor masks, each OR-combined in eight independent partial masks
           uint32_t ma = 0u, mb = 0u;
           {
@@ -780,8 +698,15 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
             ma = ((pa[0] | pa[1]) | (pa[2] | pa[3])) | ((pa[4] | pa[5]) | (pa[6] | pa[7]));
             mb = ((pb[0] | pb[1]) | (pb[2] | pb[3])) | ((pb[4] | pb[5]) | (pb[6] | pb[7]));
           }
-          if (!valid) ma = mb = 0u;  // columns past nb hold values above any bound
-          {
+          if (!valid) ma = mb = 0u;
+          // database rows beyond nb (padding of the last tile) never survive
+          if (col0 + 64 > p.nb) {
+            const int lim = p.nb - col0;
+            ma &= lim <= 0 ? 0u : (lim >= 32 ? ~0u : ((1u << lim) - 1u));
+            mb &= lim <= 32 ? 0u : (lim >= 64 ? ~0u : ((1u << (lim - 32)) - 1u));
+          }
+          if (__any_sync(0xffffffffu, (ma | mb) != 0u)) {
+            STAT_INC(st_slow, 1);
 #ifdef CURPLSH_FUSED_STATS
             {
               int mx = __popc(ma) + __popc(mb);
