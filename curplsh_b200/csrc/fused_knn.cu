@@ -258,11 +258,23 @@ __device__ __forceinline__ float thr_from(float dstar, float qn) {
 #define STAT_FLUSH(slot, acc)
 #endif
 
-// 1: an epilogue warp releases the accumulator as soon as its last TMEM read
-// of the tile has landed (before filtering that chunk); 0: after filtering.
-#ifndef CURPLSH_EARLY_RELEASE
-#define CURPLSH_EARLY_RELEASE 0
+// 1: survivor mask bits are built with set.le (all ones or zero) and one
+// lop3 that ANDs in the bit and ORs it into the partial mask (two
+// instructions a column); 0: with a compare, a select and an or.
+#ifndef CURPLSH_SET_MASKS
+#define CURPLSH_SET_MASKS 0
 #endif
+__device__ __forceinline__ uint32_t set_le_f32(float a, float b) {
+  uint32_t r;
+  asm("set.le.u32.f32 %0, %1, %2;" : "=r"(r) : "f"(a), "f"(b));
+  return r;
+}
+// (m & bit) | acc
+__device__ __forceinline__ uint32_t or_masked(uint32_t acc, uint32_t m, uint32_t bit) {
+  uint32_t r;
+  asm("lop3.b32 %0, %1, %2, %3, 0xEA;" : "=r"(r) : "r"(m), "r"(bit), "r"(acc));
+  return r;
+}
 
 // v[j] for a runtime j in [0, 32) without local memory: a 5-level select tree.
 __device__ __forceinline__ float select32(const float (&v)[32], int j) {
@@ -630,15 +642,6 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
           tmem_ld_32x32b_x64(tmem_base + lane_base + slot * kBN + g * kHalfN + h * 64, v);
           tmem_ld_wait();
           STAT_END(ttm, st_tmem);
-#if CURPLSH_EARLY_RELEASE
-          if (h == kHalfN / 64 - 1) {
-            // this warp's last TMEM read of the tile has landed: hand the
-            // accumulator back to the MMA issuer before filtering the chunk
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&acc_empty[slot]);
-          }
-#endif
           const int col0 = colh + h * 64;
           // coarse distances of the 64 columns (two independent 32-column halves)
           float da[32], db[32];
@@ -692,8 +695,13 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
             uint32_t pa[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u}, pb[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
+#if CURPLSH_SET_MASKS
+              pa[j & 7] = or_masked(pa[j & 7], set_le_f32(da[j], thr), 1u << j);
+              pb[j & 7] = or_masked(pb[j & 7], set_le_f32(db[j], thr), 1u << j);
+#else
               pa[j & 7] |= (da[j] <= thr ? 1u : 0u) << j;
               pb[j & 7] |= (db[j] <= thr ? 1u : 0u) << j;
+#endif
             }
             ma = ((pa[0] | pa[1]) | (pa[2] | pa[3])) | ((pa[4] | pa[5]) | (pa[6] | pa[7]));
             mb = ((pb[0] | pb[1]) | (pb[2] | pb[3])) | ((pb[4] | pb[5]) | (pb[6] | pb[7]));
@@ -775,11 +783,9 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
         if (MINIMA && valid)
           p.minima[(size_t)q * (2 * (size_t)p.num_tiles) + 2 * (size_t)tphys + g] =
               Tr::kFolded ? bmin : bmin + qn;
-#if !CURPLSH_EARLY_RELEASE
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(&acc_empty[slot]);
-#endif
         STAT_END(tfl, st_filter);
         }  // got
         // every S tiles (and at the unit's end) meet the partner warp; leave

@@ -47,10 +47,12 @@ def _search(cb, res, base, queries, k, form, which="coarse"):
 
 
 def test_fp8_on_integer_mixture_is_exact_with_the_check(env):
-    """The integer Gaussian mixture of the 1M-row workload at N = 200,000."""
+    """The 1M-row integer Gaussian mixture (its first 256 queries): ~1,000
+    rows per cluster, so a query's 100th and 400th neighbours lie ~5,000
+    apart while FP8's coarse error is ~10,000."""
     cb, res = env
     s = _synth()
-    base, queries = s.mixture_int(200_000, 256)
+    base, queries, _ = s.make("mixture_int_1m", q=256)
     k = 100
     rd, ri = oracle.knn(base, queries, k + 1)
     cb.set_coarse_check(True)
