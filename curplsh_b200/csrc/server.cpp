@@ -40,6 +40,7 @@
 #include "../../include/curplsh_b200.h"
 #include "fused_knn.h"
 #include "multi_plan.h"
+#include "server_sched.h"
 
 using namespace curplsh_b200;
 
@@ -68,54 +69,6 @@ int pointer_dev(const void* p) {
   }
   return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) ? a.device : -1;
 }
-
-// First-fit allocator over [0, size) with coalescing; 256-byte granules.
-class Arena {
- public:
-  void reset(size_t size) {
-    free_.clear();
-    free_[0] = size;
-    size_ = size;
-    in_use_ = 0;
-  }
-  bool alloc(size_t bytes, size_t* off) {
-    bytes = rup(bytes, 256);
-    for (auto it = free_.begin(); it != free_.end(); ++it) {
-      if (it->second >= bytes) {
-        *off = it->first;
-        const size_t rest = it->second - bytes, start = it->first + bytes;
-        free_.erase(it);
-        if (rest) free_[start] = rest;
-        in_use_ += bytes;
-        return true;
-      }
-    }
-    return false;
-  }
-  void release(size_t off, size_t bytes) {
-    bytes = rup(bytes, 256);
-    in_use_ -= bytes;
-    auto it = free_.emplace(off, bytes).first;
-    auto nx = std::next(it);
-    if (nx != free_.end() && it->first + it->second == nx->first) {
-      it->second += nx->second;
-      free_.erase(nx);
-    }
-    if (it != free_.begin()) {
-      auto pv = std::prev(it);
-      if (pv->first + pv->second == it->first) {
-        pv->second += it->second;
-        free_.erase(it);
-      }
-    }
-  }
-  size_t in_use() const { return in_use_; }
-  size_t size() const { return size_; }
-
- private:
-  std::map<size_t, size_t> free_;
-  size_t size_ = 0, in_use_ = 0;
-};
 
 enum ReqState { kPending = 0, kRunning = 1, kDone = 2, kFailed = 3 };
 
@@ -269,14 +222,8 @@ bool issue_step(curplsh_server* s, std::unique_lock<std::mutex>& lk) {
   if (slot_i < 0 || s->pending.empty()) return false;
   Slot& slot = s->slots[slot_i];
   // take requests first come, first served within the per-step query cap
-  std::vector<int64_t> take;
-  int64_t q = 0;
-  for (int64_t t : s->pending) {
-    const Request& r = s->reqs[t];
-    if (!take.empty() && q + r.num > s->cfg.max_step_queries) break;
-    take.push_back(t);
-    q += r.num;
-  }
+  std::vector<int64_t> take =
+      take_step(s->pending, s->cfg.max_step_queries, [&](int64_t t) { return s->reqs[t].num; });
   std::vector<curplsh_index*> uniq{s->index};
   std::vector<IndexView> views(1);
   if (index_lock_view(s->index, &views[0])) return false;
@@ -286,17 +233,18 @@ bool issue_step(curplsh_server* s, std::unique_lock<std::mutex>& lk) {
   std::vector<curplsh_batch_item> items;
   size_t staging = 0;
   int rc = CURPLSH_OK;
-  // shrink the step until its working memory fits the free arena
-  for (;;) {
-    rc = build_step(s, take, uniq, views, st->plan, items, &staging);
-    if (rc) break;
-    st->bytes = rup(st->plan.bytes(), 256) + staging;
-    if (s->arena.alloc(st->bytes, &st->off)) break;
-    if (take.size() == 1) {
-      index_unlock(s->index);
-      return false;  // admission: wait for running steps to release memory
-    }
-    take.resize(take.size() / 2);
+  // shrink the step until its working memory fits the free arena (the plan
+  // and items left behind are those of the admitted requests)
+  const int adm = admit_step(take, s->arena, &st->off, &st->bytes,
+                             [&](const std::vector<int64_t>& tk, size_t* bytes) -> int {
+                               rc = build_step(s, tk, uniq, views, st->plan, items, &staging);
+                               if (rc) return rc;
+                               *bytes = rup(st->plan.bytes(), 256) + staging;
+                               return 0;
+                             });
+  if (adm == 0) {
+    index_unlock(s->index);
+    return false;  // admission: wait for running steps to release memory
   }
   if (rc) {
     index_unlock(s->index);
@@ -393,6 +341,8 @@ bool issue_step(curplsh_server* s, std::unique_lock<std::mutex>& lk) {
   }
   s->stats.steps += 1;
   s->stats.kernel_launches += kernels;
+  int64_t q = 0;
+  for (int64_t t : take) q += s->reqs[t].num;
   if (q > s->stats.max_step_queries) s->stats.max_step_queries = q;
   s->inflight.push_back(std::move(st));
   if ((int)s->inflight.size() > s->stats.max_inflight_seen) s->stats.max_inflight_seen = (int)s->inflight.size();

@@ -62,3 +62,19 @@ def test_cpp_device_memory_reservations(tmp_path):
     r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "cpp device memory ok" in r.stdout
+
+
+def test_server_admission_and_step_forming(tmp_path):
+    """The serving loop's scheduling rules (curplsh_b200/csrc/server_sched.h):
+    first-fit arena with coalescing, first-come-first-served steps under the
+    query cap, and halving a step until its memory fits -- on the host."""
+    cxx = shutil.which("g++")
+    if not cxx:
+        pytest.skip("g++ not available")
+    exe = str(tmp_path / "ts")
+    r = subprocess.run([cxx, "-std=c++17", "-O2", "-Wall", "-I", os.path.join(ROOT, "curplsh_b200", "csrc"),
+                        os.path.join(ROOT, "tests", "cpp", "test_server_sched.cpp"), "-o", exe],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and "server sched ok" in r.stdout, r.stdout + r.stderr
