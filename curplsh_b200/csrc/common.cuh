@@ -67,16 +67,13 @@ constexpr int kBM = 128;          // queries per block: MMA M, one TMEM lane per
 constexpr int kBN = 256;          // database rows per tile: MMA N (TMEM columns per accumulator)
 constexpr int kHalfN = kBN / 2;   // columns of a tile handled by one epilogue warpgroup
 constexpr int kChunkBytes = 128;  // K extent of one smem chunk row (one 128-byte swizzle atom)
-// Threads of a fused CTA: warp 0 TMA producer, warp 1 MMA issuer, then the
-// epilogue warps (fused_threads below).
+constexpr int kNumThreads = 320;  // warp 0 TMA producer, warp 1 MMA issuer, warps 2..9 epilogue
 // BF16 forms append kAugCols columns to every row so the tensor cores add the
 // norms: database rows carry [n1 n2 n3 1 1 1] (||x||^2 = n1+n2+n3, three BF16
 // terms), query rows (stored as -2q) carry [1 1 1 m1 m2 m3] (||q||^2 = m1+m2+m3),
 // and the accumulator is ||q||^2 + ||x||^2 - 2 q.x directly.
 constexpr int kAugCols = 6;
-constexpr int kEpiWarps = 8;       // epilogue warps of the FP32-exact form and the block-minimum pass
-constexpr int kEpiWarpsWide = 16;  // epilogue warps of the BF16 and FP8 forms (four per SM sub-partition)
-__host__ __device__ constexpr int fused_threads(int epi_warps) { return 64 + 32 * epi_warps; }
+constexpr int kEpiWarps = 8;
 constexpr int kPoolRoom = kBN;  // free slots a candidate pool keeps for the next tile (both halves)
 // Tiles between two selection points of a shared candidate pool: two when the
 // capacity leaves room for two tiles of appends above k' + 128, else one.

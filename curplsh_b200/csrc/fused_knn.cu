@@ -95,7 +95,7 @@ struct SmemLayout {
   uint32_t total;      // dynamic smem bytes requested (includes 1 KB alignment slack)
 };
 
-__host__ __device__ inline SmemLayout make_layout(int form, int d, int epi_warps) {
+__host__ __device__ inline SmemLayout make_layout(int form, int d) {
   SmemLayout L{};
   const bool folded = form != kFormFP8;
   const int chunk_elems = folded ? 64 : 128;
@@ -107,7 +107,7 @@ __host__ __device__ inline SmemLayout make_layout(int form, int d, int epi_warps
   // the tail runs the hi x hi product alone, which is exact only for those
   L.tail_narrow = folded && (d % 64 == 0);
   // everything below the barrier block must fit the 227 KB opt-in limit
-  const uint32_t budget = 227u * 1024u - 256u - (uint32_t)epi_warps * 256u * 4u - 1024u - 1024u;
+  const uint32_t budget = 227u * 1024u - 256u - (uint32_t)kEpiWarps * 256u * 4u - 1024u - 1024u;
   const int nreg = L.nkc - (L.tail_narrow ? 1 : 0);
   const uint32_t a_res = (uint32_t)nreg * a_parts * kAChunkBytes + (L.tail_narrow ? kATailBytes : 0u);
   // a stage = one regular K chunk of the tile; the last one also carries the tail
@@ -126,7 +126,7 @@ __host__ __device__ inline SmemLayout make_layout(int form, int d, int epi_warps
   L.stages = s < 2 ? 2 : (s > 8 ? 8 : s);
   L.bar_off = L.a_bytes + (uint32_t)L.stages * L.stage_bytes;
   L.hist_off = L.bar_off + 256;  // barriers: 2*8 + 6 mbarriers + tmem slot + flags < 256 B
-  L.pool_off = L.hist_off + epi_warps * 256 * 4;
+  L.pool_off = L.hist_off + kEpiWarps * 256 * 4;
   L.total = L.pool_off + 1024 + 1024;
   return L;
 }
@@ -294,10 +294,8 @@ __device__ __forceinline__ float select32(const float (&v)[32], int j) {
 // MINIMA selects the block-minimum mode (FusedItem::minima, the sample pass of
 // the bound estimate) at compile time, so the candidate-pool kernel carries
 // none of its code.
-template <int FORM, int MAXI, bool MINIMA, int EPI>
-__global__ void __launch_bounds__(fused_threads(EPI), 1) fused_knn_kernel(const __grid_constant__ FusedArgs<MAXI> A) {
-  static_assert(EPI == 8 || EPI == 16, "8 or 16 epilogue warps");
-  static_assert(!MINIMA || EPI == 8, "the block-minimum layout has one minimum per 128-row half tile");
+template <int FORM, int MAXI, bool MINIMA = false>
+__global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_constant__ FusedArgs<MAXI> A) {
   using Tr = FormTraits<FORM>;
   const FusedBatch& B = A.B;
   // a conditional pass (a re-search after a failed check): every thread of
@@ -306,7 +304,7 @@ __global__ void __launch_bounds__(fused_threads(EPI), 1) fused_knn_kernel(const 
   if (B.run_if && *B.run_if == 0) return;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const SmemLayout L = make_layout(FORM, B.d, EPI);
+  const SmemLayout L = make_layout(FORM, B.d);
   const int S = L.stages;
 
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.bar_off);
@@ -334,7 +332,7 @@ __global__ void __launch_bounds__(fused_threads(EPI), 1) fused_knn_kernel(const 
     mbar_init(a_empty, 1);
     for (int s = 0; s < 2; ++s) {
       mbar_init(&acc_full[s], 1);
-      mbar_init(&acc_empty[s], EPI);
+      mbar_init(&acc_empty[s], kEpiWarps);
     }
     mbar_init(drain, 1);
     *abort_flag = 0;
@@ -507,23 +505,18 @@ __global__ void __launch_bounds__(fused_threads(EPI), 1) fused_knn_kernel(const 
     }
   } else {
     // ------------------------------------------------------------ epilogue
-    // Warps ew, ew + 4, ... read the same TMEM lanes (queries) and split each
-    // tile's columns into kParts parts g = 0 .. kParts-1 (128 columns each with
-    // 8 epilogue warps, 64 with 16: four warps per SM sub-partition hide more
-    // of the compare chains' latency).  They share ONE candidate pool per
+    // Warps ew and ew + 4 read the same TMEM lanes (queries) and split each
+    // tile's columns into halves g = 0, 1.  They share ONE candidate pool per
     // (query, unit): appends reserve slots with a shared-memory counter, and at
-    // every tile end the group meets at a named barrier, splits the pools that
+    // every tile end the pair meets at a named barrier, splits the pools that
     // need a selection between them, and meets again.  A shared pool sees
-    // every part's rows, so its bound tightens as one pool over the whole
-    // tile would -- far fewer survivors and selections than a pool per part.
-    constexpr int kParts = EPI / 4;
-    constexpr int kPartCols = kBN / kParts;
-    constexpr int kGroupThreads = 32 * kParts;
-    const int ew = warp - 2;       // 0 .. EPI-1
-    const int g = ew >> 2;         // which column part of each tile
+    // both halves' rows, so its bound tightens as one pool over the whole
+    // tile would -- about half the survivors and selections of a pool per half.
+    const int ew = warp - 2;       // 0..7
+    const int g = ew >> 2;         // which 128-column half of each tile
     const int lg = warp & 3;       // TMEM lane group this warp may access
     const int row = lg * 32 + lane;
-    const int pair_bar = 1 + lg;   // named barrier of the warps of lane group lg
+    const int pair_bar = 1 + lg;   // named barrier of the two warps of lane group lg
     uint32_t* hist = hist_all + ew * 256;
     int* cnt_s = reinterpret_cast<int*>(smem + L.pool_off);             // [128] pool counts
     float* thr_s = reinterpret_cast<float*>(smem + L.pool_off) + kBM;   // [128] pool bounds
@@ -550,7 +543,7 @@ __global__ void __launch_bounds__(fused_threads(EPI), 1) fused_knn_kernel(const 
       const int P = p.pool_cap;
       const int U = p.units_per_block;
       const int S = pool_sync_tiles(P, p.kprime);
-      if (u_ord < 0 || u_ord >= U) {  // identical in every epilogue warp: the whole group leaves here
+      if (u_ord < 0 || u_ord >= U) {  // identical in every epilogue warp: both of a pair leave here
         raise_abort(abort_flag, B.status, kErrBadSchedule);
         break;
       }
@@ -570,12 +563,12 @@ __global__ void __launch_bounds__(fused_threads(EPI), 1) fused_knn_kernel(const 
         cnt_s[row] = 0;
         thr_s[row] = 3.402823466e38f;
       }
-      bar_sync_named(pair_bar, kGroupThreads);
+      bar_sync_named(pair_bar, 64);
       float thr = 3.402823466e38f;  // FLT_MAX: admits every finite distance until a pool fills
 
       // Selections of the pools in `need` (lane bits of this lane group; warp g
-      // owns the pools of lanes l with l % kParts == g, so no two warps of the
-      // group touch the same pool's state).  Each keeps `keep` keys, records the pool's new
+      // owns the pools of lanes with parity g, so the pair never touches the
+      // same pool's state).  Each keeps `keep` keys, records the pool's new
       // count and bound in shared memory and publishes a full set's k'-th
       // distance to q_bound.
       auto refresh = [&](uint32_t need, int keep) {
@@ -608,15 +601,15 @@ __global__ void __launch_bounds__(fused_threads(EPI), 1) fused_knn_kernel(const 
         thr = fminf(thr, thr_s[row]);
         if (nb_ob != kOrdInf) thr = fminf(thr, thr_from<Tr::kFolded>(ord2f(nb_ob), qn));
         if (valid) nb_ob = ld_relaxed_u32(&p.q_bound[q]);
-        // FP8: this part's database norms and scales, loaded before the
+        // FP8: this half tile's database norms and scales, loaded before the
         // accumulator wait (their latency overlaps it) and staged in the
         // warp's histogram area, which is free outside a refresh
-        float pxn[kPartCols / 32], psx[kPartCols / 32];
+        float pxn[4], psx[4];
         if (Tr::kFP8) {
 #pragma unroll
-          for (int i = 0; i < kPartCols / 32; ++i) {
+          for (int i = 0; i < 4; ++i) {
             // < nb_pad: rows are padded to whole tiles (a strided sample has no padding)
-            const int c0 = tphys * kBN + g * kPartCols + lane + 32 * i;
+            const int c0 = tphys * kBN + g * kHalfN + lane + 32 * i;
             const size_t c = MINIMA ? (size_t)c0 * (size_t)p.db_step : (size_t)c0;
             pxn[i] = __ldg(p.db_norms + c);
             psx[i] = __ldg(p.db_scale + c);
@@ -626,120 +619,27 @@ __global__ void __launch_bounds__(fused_threads(EPI), 1) fused_knn_kernel(const 
         bool got = wait_or_abort(&acc_full[slot], use & 1u, abort_flag);
         if (!got) raise_abort(abort_flag, B.status, kErrWaitTimeout);
         STAT_END(tw, st_wait);
-        // an aborting warp skips the tile but still meets its group below
+        // an aborting warp skips the tile but still meets its partner below
         if (got) {
         STAT_BEGIN(tfl);
         tc_fence_after();
-        const int colh = tphys * kBN + g * kPartCols;
+        const int colh = tphys * kBN + g * kHalfN;
         float bmin = 3.402823466e38f;  // block-minimum mode: smallest distance of this half tile
-        float* colv = reinterpret_cast<float*>(hist);  // [kPartCols] norms, then [kPartCols] scales
+        float* colv = reinterpret_cast<float*>(hist);  // [128] norms, then [128] scales
         if (Tr::kFP8) {
           __syncwarp();
 #pragma unroll
-          for (int i = 0; i < kPartCols / 32; ++i) {
+          for (int i = 0; i < 4; ++i) {
             colv[lane + 32 * i] = pxn[i];
-            colv[kPartCols + lane + 32 * i] = psx[i];
+            colv[kHalfN + lane + 32 * i] = psx[i];
           }
           __syncwarp();
         }
-        if constexpr (EPI == 16) {
 #pragma unroll 1
-        for (int h = 0; h < kPartCols / 32; ++h) {
-          // 32-column chunks: with four warps per SM sub-partition a thread
-          // has ~100 registers, too few to hold 64 columns and their masks
-          uint32_t v[32];
-          STAT_BEGIN(ttm);
-          tmem_ld_32x32b_x32(tmem_base + lane_base + slot * kBN + g * kPartCols + h * 32, v);
-          tmem_ld_wait();
-          STAT_END(ttm, st_tmem);
-          const int col0 = colh + h * 32;
-          float da[32];
-          if (Tr::kFolded) {
-#pragma unroll
-            for (int j = 0; j < 32; ++j) da[j] = __uint_as_float(v[j]);
-          } else {
-            const float4* xn4 = reinterpret_cast<const float4*>(colv + h * 32);
-            const float4* sx4 = reinterpret_cast<const float4*>(colv + kPartCols + h * 32);
-#pragma unroll
-            for (int j4 = 0; j4 < 8; ++j4) {
-              const float4 xn = xn4[j4];
-              const float4 sx = sx4[j4];
-              float p0, p1, p2, p3;
-              mul2_f32(p0, p1, __uint_as_float(v[4 * j4 + 0]), __uint_as_float(v[4 * j4 + 1]), sx.x, sx.y);
-              mul2_f32(p2, p3, __uint_as_float(v[4 * j4 + 2]), __uint_as_float(v[4 * j4 + 3]), sx.z, sx.w);
-              fma2_f32(da[4 * j4 + 0], da[4 * j4 + 1], p0, p1, m2s, m2s, xn.x, xn.y);
-              fma2_f32(da[4 * j4 + 2], da[4 * j4 + 3], p2, p3, m2s, m2s, xn.z, xn.w);
-            }
-          }
-          uint32_t ma = 0u;
-          {
-            uint32_t pa[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
-#pragma unroll
-            for (int j = 0; j < 32; ++j) {
-#if CURPLSH_SET_MASKS
-              pa[j & 7] = or_masked(pa[j & 7], set_le_f32(da[j], thr), 1u << j);
-#else
-              pa[j & 7] |= (da[j] <= thr ? 1u : 0u) << j;
-#endif
-            }
-            ma = ((pa[0] | pa[1]) | (pa[2] | pa[3])) | ((pa[4] | pa[5]) | (pa[6] | pa[7]));
-          }
-          if (!valid) ma = 0u;
-          // database rows beyond nb (padding of the last tile) never survive
-          if (col0 + 32 > p.nb) {
-            const int lim = p.nb - col0;
-            ma &= lim <= 0 ? 0u : (lim >= 32 ? ~0u : ((1u << lim) - 1u));
-          }
-          if (__any_sync(0xffffffffu, ma != 0u)) {
-            STAT_INC(st_slow, 1);
-            int n = 0;
-            {
-              const int c = __popc(ma);
-              if (c) n = atomicAdd(&cnt_s[row], c);
-            }
-            if (ma == ~0u) {
-              // every column survives (a pool with no bound yet)
-#pragma unroll
-              for (int j = 0; j < 32; ++j)
-                if (n + j < P) pool[n + j] = make_key(Tr::kFolded ? da[j] : da[j] + qn, (uint32_t)(col0 + j));
-              n += 32;
-              ma = 0u;
-              STAT_INC(st_surv, 32);
-            }
-            auto take = [&]() {
-              if (ma) {
-                const int j = __ffs(ma) - 1;
-                ma &= ma - 1;
-                const float x = select32(da, j);
-                if (n < P) pool[n] = make_key(Tr::kFolded ? x : x + qn, (uint32_t)(col0 + j));
-                ++n;
-                STAT_INC(st_surv, 1);
-              }
-            };
-            take();
-            if (__any_sync(0xffffffffu, ma != 0u)) {
-              take();
-              if (__any_sync(0xffffffffu, ma != 0u)) {
-                float stash[32];
-#pragma unroll
-                for (int j = 0; j < 32; ++j) stash[j] = da[j];
-                while (ma) {
-                  const int j = __ffs(ma) - 1;
-                  ma &= ma - 1;
-                  if (n < P) pool[n] = make_key(Tr::kFolded ? stash[j] : stash[j] + qn, (uint32_t)(col0 + j));
-                  ++n;
-                  STAT_INC(st_surv, 1);
-                }
-              }
-            }
-          }
-        }
-        } else {
-#pragma unroll 1
-        for (int h = 0; h < kPartCols / 64; ++h) {
+        for (int h = 0; h < kHalfN / 64; ++h) {
           uint32_t v[64];
           STAT_BEGIN(ttm);
-          tmem_ld_32x32b_x64(tmem_base + lane_base + slot * kBN + g * kPartCols + h * 64, v);
+          tmem_ld_32x32b_x64(tmem_base + lane_base + slot * kBN + g * kHalfN + h * 64, v);
           tmem_ld_wait();
           STAT_END(ttm, st_tmem);
           const int col0 = colh + h * 64;
@@ -754,7 +654,7 @@ __global__ void __launch_bounds__(fused_threads(EPI), 1) fused_knn_kernel(const 
             }
           } else {
             const float4* xn4 = reinterpret_cast<const float4*>(colv + h * 64);
-            const float4* sx4 = reinterpret_cast<const float4*>(colv + kPartCols + h * 64);
+            const float4* sx4 = reinterpret_cast<const float4*>(colv + kHalfN + h * 64);
 #pragma unroll
             for (int j4 = 0; j4 < 16; ++j4) {
               const float4 xn = xn4[j4];
@@ -880,7 +780,6 @@ __global__ void __launch_bounds__(fused_threads(EPI), 1) fused_knn_kernel(const 
             }
           }
         }
-        }
         if (MINIMA && valid)
           p.minima[(size_t)q * (2 * (size_t)p.num_tiles) + 2 * (size_t)tphys + g] =
               Tr::kFolded ? bmin : bmin + qn;
@@ -889,26 +788,26 @@ __global__ void __launch_bounds__(fused_threads(EPI), 1) fused_knn_kernel(const 
         if (lane == 0) mbar_arrive(&acc_empty[slot]);
         STAT_END(tfl, st_filter);
         }  // got
-        // every S tiles (and at the unit's end) meet the group's other warps;
-        // leave together if any of them aborted
+        // every S tiles (and at the unit's end) meet the partner warp; leave
+        // together if either aborted
         if ((t - t0 + 1) % S != 0 && t + 1 < t1) continue;
         STAT_BEGIN(tb1);
-        const bool leave = bar_red_or(pair_bar, kGroupThreads, !got || *abort_flag != 0);
+        const bool leave = bar_red_or(pair_bar, 64, !got || *abort_flag != 0);
         STAT_END(tb1, st_bar);
         if (leave) {
           ok = false;
           break;
         }
-        // pools that may not have room for the next S tiles (all parts),
+        // pools that may not have room for the next S tiles (both halves),
         // or, at the unit's end, every pool above k' (the merge pass reads at
         // most k' keys' worth beyond what it needs)
         const int lim = t + 1 < t1 ? P - S * kBN : p.kprime;
-        const bool mine = (lane % kParts) == g;
+        const bool mine = (lane & 1) == g;
         const int cn = mine ? cnt_s[row] : 0;
         if (cn > P) atomicOr(B.status, kErrPoolOverflow);
         refresh(__ballot_sync(0xffffffffu, mine && valid && cn > lim), p.kprime);
         STAT_BEGIN(tb2);
-        bar_sync_named(pair_bar, kGroupThreads);
+        bar_sync_named(pair_bar, 64);
         STAT_END(tb2, st_bar);
       }
       if (!ok) break;
@@ -919,7 +818,7 @@ __global__ void __launch_bounds__(fused_threads(EPI), 1) fused_knn_kernel(const 
         p.pool_counts[(pool_row0 + row) * U + u_ord] = cn < P ? cn : P;
         if (gap) p.pool_counts[(pool_row0 + row) * U + u_ord - 1] = 0;
       }
-      bar_sync_named(pair_bar, kGroupThreads);  // the counts are read before the next unit resets them
+      bar_sync_named(pair_bar, 64);  // the counts are read before the next unit resets them
     }
     if (lane == 0) {
       STAT_FLUSH(kStatEpiWaitAccFull, st_wait);
@@ -983,20 +882,6 @@ bool make_map(CUtensorMap* m, const void* base, bool fp8, long long rows, long l
   return r == CUDA_SUCCESS;
 }
 
-// Epilogue warps of a kernel instance: the BF16 and FP8 pools are filtered by
-// 16 warps (their epilogue bounds the pass), the FP32-exact form (bounded by
-// its three products) and the block-minimum pass by 8.
-#ifndef CURPLSH_WIDE_EPI
-#define CURPLSH_WIDE_EPI 1
-#endif
-template <int FORM, bool MINIMA>
-constexpr int epi_of() {
-  return (FORM == kFormExact || MINIMA || !CURPLSH_WIDE_EPI) ? kEpiWarps : kEpiWarpsWide;
-}
-inline int epi_warps_for(int form, bool minima) {
-  return (form == kFormExact || minima || !CURPLSH_WIDE_EPI) ? kEpiWarps : kEpiWarpsWide;
-}
-
 // Raises the kernel's dynamic shared memory limit once per device.
 template <int FORM, int MAXI, bool MINIMA = false>
 cudaError_t ensure_attributes() {
@@ -1004,8 +889,8 @@ cudaError_t ensure_attributes() {
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr_done[dev & 63]) {
-    cudaError_t e = cudaFuncSetAttribute(fused_knn_kernel<FORM, MAXI, MINIMA, epi_of<FORM, MINIMA>()>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaError_t e = cudaFuncSetAttribute(fused_knn_kernel<FORM, MAXI, MINIMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         227 * 1024);
     if (e != cudaSuccess) return e;
     attr_done[dev & 63] = true;
   }
@@ -1077,8 +962,7 @@ cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, 
       m[kMapXTail] = m[kMapXHi];
     }
   }
-  constexpr int EPI = epi_of<FORM, MINIMA>();
-  fused_knn_kernel<FORM, MAXI, MINIMA, EPI><<<bp.grid, fused_threads(EPI), smem, st>>>(a);
+  fused_knn_kernel<FORM, MAXI, MINIMA><<<bp.grid, kNumThreads, smem, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -1145,7 +1029,7 @@ void plan_fused(int nq, int nb, int num_sms, FusedPlan* out, int split_q4) {
   out->split_tiles = ip.split_tiles;
 }
 
-uint32_t fused_smem_bytes(int form, int d) { return make_layout(form, d, epi_warps_for(form, false)).total; }
+uint32_t fused_smem_bytes(int form, int d) { return make_layout(form, d).total; }
 
 cudaError_t prepare_fused_kernels(int form) {
   cudaError_t e;
@@ -1171,7 +1055,7 @@ cudaError_t launch_fused_batch(int form, const FusedItemSpec* specs, const Fused
   for (int i = 1; i < n; ++i)
     if (specs[i].d != specs[0].d) return cudaErrorInvalidValue;
   if (bp.grid == 0) return cudaSuccess;
-  const uint32_t smem = make_layout(form, specs[0].d, epi_warps_for(form, specs[0].minima != nullptr)).total;
+  const uint32_t smem = make_layout(form, specs[0].d).total;
   if (smem > 227u * 1024u) return cudaErrorInvalidConfiguration;  // a layout bug, not a caller error
   switch (form) {
     case kFormExact:

@@ -29,7 +29,10 @@ namespace {
 constexpr int kMergeThreads = 256;
 // Candidates one warp reranks at once: each lane keeps this many database rows
 // in flight (a row of d = 128 is one 16-byte load per lane).
-constexpr int kRerankRows = 8;
+#ifndef CURPLSH_RERANK_ROWS
+#define CURPLSH_RERANK_ROWS 4
+#endif
+constexpr int kRerankRows = CURPLSH_RERANK_ROWS;
 
 __device__ __forceinline__ uint32_t block_incl_scan(uint32_t v, uint32_t* warp_tot) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
