@@ -265,7 +265,7 @@ class IndexBFConfig:
     """IndexBFConfig (include/index_bf.h:8-19) + IndexConfig (include/index.h:8-16) + precision controls."""
 
     def __init__(self, device=0, memorySpace=MemorySpace.Device, storeTransposed=False,
-                 computeExactDistances=False, precision=Precision.FP32_EXACT, rerankFactor=4,
+                 computeExactDistances=False, precision=Precision.FP32_EXACT, rerankFactor=0,
                  borrowDeviceData=False):
         self.device = device
         self.memorySpace = memorySpace
@@ -577,15 +577,16 @@ class Server:
         return lat.value
 
     def wait_phases(self, ticket: int, timeout: float = -1.0):
-        """wait() that also returns the latency's phases (seconds, host clock):
-        (latency, waiting for a step, step on the device, retiring)."""
+        """wait() that also returns the latency's phases (seconds): (latency,
+        waiting for a step, step on the device, retiring) on the host clock,
+        and the step's device work itself timed by CUDA events."""
         lat = ctypes.c_double(0.0)
-        ph = (ctypes.c_double * 3)()
+        ph = (ctypes.c_double * 4)()
         rc = _lib.curplsh_server_wait_phases(self._h, int(ticket), float(timeout), ctypes.byref(lat), ph)
         if rc != ERR_STATE:
             self._keep.pop(ticket, None)
         _check(rc)
-        return lat.value, ph[0], ph[1], ph[2]
+        return lat.value, ph[0], ph[1], ph[2], ph[3]
 
     def stats(self) -> dict:
         st = _ServerStats()

@@ -82,6 +82,7 @@ struct Request {
   // host clock: submitted, issued in a step, the step's completion callback
   // ran, results visible to wait()
   double t_submit = 0, t_issue = 0, t_gpu = 0, t_done = 0;
+  double gpu_exec = 0;  // seconds between the step's first and last work on its stream (CUDA events)
   int state = kPending;
   int err = CURPLSH_OK;
   std::string msg;
@@ -93,6 +94,7 @@ struct Slot {
   char* pinned = nullptr;  // host staging: queries, then outputs, then the status word
   size_t pinned_bytes = 0;
   bool busy = false;
+  cudaEvent_t ev_begin = nullptr, ev_end = nullptr;  // bracket the step's device work on st
 };
 
 struct Step {
@@ -183,6 +185,11 @@ void finish_step(curplsh_server* s, Step& st) {
   // called with the lock held, after the step's stream has completed
   const Slot& slot = s->slots[st.slot];
   const uint32_t status = *reinterpret_cast<const uint32_t*>(slot.pinned + slot.pinned_bytes - 256);
+  float exec_ms = 0.f;
+  if (cudaEventElapsedTime(&exec_ms, slot.ev_begin, slot.ev_end) != cudaSuccess) {
+    cudaGetLastError();
+    exec_ms = 0.f;
+  }
   for (auto& ho : st.host_out) {
     Request& r = s->reqs[ho.first];
     const size_t ni = (size_t)r.num * r.k;
@@ -194,6 +201,7 @@ void finish_step(curplsh_server* s, Step& st) {
     Request& r = s->reqs[tk];
     r.t_done = t;
     r.t_gpu = st.t_gpu_done;
+    r.gpu_exec = exec_ms * 1e-3;
     if (status) {
       r.state = kFailed;
       r.err = CURPLSH_ERR_DEVICE;
@@ -272,7 +280,7 @@ bool issue_step(curplsh_server* s, std::unique_lock<std::mutex>& lk) {
   size_t doff = rup(st->plan.bytes(), 256);
   size_t pq = 0;                        // pinned query cursor
   size_t po = pinned_query_bytes(s);     // pinned output cursor
-  cudaError_t e = cudaSuccess;
+  cudaError_t e = cudaEventRecord(slot.ev_begin, slot.st);
   for (size_t i = 0; i < take.size(); ++i) {
     Request& r = s->reqs[take[i]];
     curplsh_batch_item& it = items[i];
@@ -316,6 +324,7 @@ bool issue_step(curplsh_server* s, std::unique_lock<std::mutex>& lk) {
   if (!rc && e == cudaSuccess)
     e = cudaMemcpyAsync(slot.pinned + slot.pinned_bytes - 256, st->plan.status(), sizeof(uint32_t),
                         cudaMemcpyDeviceToHost, slot.st);
+  if (!rc && e == cudaSuccess) e = cudaEventRecord(slot.ev_end, slot.st);
   if (!rc && e == cudaSuccess) e = cudaLaunchHostFunc(slot.st, on_step_done, st.get());
   if (rc || e != cudaSuccess) {
     if (e != cudaSuccess) {
@@ -426,6 +435,8 @@ int curplsh_server_create(curplsh_index* index, const curplsh_server_config* cfg
     e = cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking);
     sl.pinned_bytes = pinned_bytes_for(s.get());
     if (e == cudaSuccess) e = cudaMallocHost(&sl.pinned, sl.pinned_bytes);
+    if (e == cudaSuccess) e = cudaEventCreate(&sl.ev_begin);
+    if (e == cudaSuccess) e = cudaEventCreate(&sl.ev_end);
     s->slots.push_back(sl);
   }
   for (int form = 0; form < 3 && e == cudaSuccess; ++form) e = prepare_fused_kernels(form);
@@ -435,6 +446,8 @@ int curplsh_server_create(curplsh_index* index, const curplsh_server_config* cfg
     for (Slot& sl : s->slots) {
       if (sl.st) cudaStreamDestroy(sl.st);
       if (sl.pinned) cudaFreeHost(sl.pinned);
+      if (sl.ev_begin) cudaEventDestroy(sl.ev_begin);
+      if (sl.ev_end) cudaEventDestroy(sl.ev_end);
     }
     if (s->arena_mem) cudaFree(s->arena_mem);
     restore();
@@ -524,6 +537,7 @@ int curplsh_server_wait_phases(curplsh_server* s, int64_t ticket, double timeout
     phases[0] = r.t_issue > 0 ? r.t_issue - r.t_submit : r.t_done - r.t_submit;  // waiting for a step
     phases[1] = ran ? r.t_gpu - r.t_issue : 0.0;                                 // step issued -> GPU done
     phases[2] = ran ? r.t_done - r.t_gpu : 0.0;                                  // GPU done -> visible
+    phases[3] = ran ? r.gpu_exec : 0.0;  // the step's device work itself (CUDA events, inside phases[1])
   }
   if (r.state == kFailed) return fail(r.err ? r.err : CURPLSH_ERR_DEVICE, "%s", r.msg.c_str());
   return CURPLSH_OK;
@@ -556,6 +570,8 @@ int curplsh_server_destroy(curplsh_server* s) {
     cudaStreamSynchronize(sl.st);
     cudaStreamDestroy(sl.st);
     cudaFreeHost(sl.pinned);
+    cudaEventDestroy(sl.ev_begin);
+    cudaEventDestroy(sl.ev_end);
   }
   cudaFree(s->arena_mem);
   cudaSetDevice(prev);

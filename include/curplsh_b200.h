@@ -60,13 +60,14 @@ typedef struct curplsh_bf_config {
   int32_t compute_exact_distances; /* IndexBFConfig::computeExactDistances: IndexBF::search always
                                       returns exact squared distances (src/index_bf.cpp:68-69), so is this */
   int32_t precision;               /* CURPLSH_PRECISION_* default for search */
-  int32_t rerank_factor;           /* k' = rerank_factor * k for the BF16/FP8 forms (default 4) */
+  int32_t rerank_factor;           /* k' = rerank_factor * k for the BF16/FP8 forms; 0 (default): 4 for
+                                      BF16, 32 for FP8 (E4M3's coarse error needs the wider margin) */
   int32_t borrow_device_data;      /* 1: add() of device memory keeps a reference to the caller's FP32
                                       rows (the reference's aliasing, include/device_tensor.h:97-103);
                                       0 (default): the index copies them */
 } curplsh_bf_config;
 
-/* Defaults: device 0, device memory, FP32-exact, rerank_factor 4, copy on add. */
+/* Defaults: device 0, device memory, FP32-exact, rerank_factor 0 (the form's default), copy on add. */
 void curplsh_bf_config_init(curplsh_bf_config* cfg);
 
 const char* curplsh_last_error(void);
@@ -244,9 +245,11 @@ int curplsh_server_submit(curplsh_server* server, int64_t num, const float* quer
  * returns its status and, when latency_s is not NULL, seconds from submit to completion.  A ticket
  * can be waited for once. */
 int curplsh_server_wait(curplsh_server* server, int64_t ticket, double timeout_s, double* latency_s);
-/* curplsh_server_wait that also splits the latency (host clock) into phases[3]: waiting for a
+/* curplsh_server_wait that also splits the latency (host clock) into phases[0..2]: waiting for a
  * step (submit to issue), the step on the device (issue to its completion callback), and
- * retiring (callback to the results being visible to wait).  No counterpart in the reference. */
+ * retiring (callback to the results being visible to wait); phases[3] is the step's device work
+ * itself, timed by CUDA events around it on its stream (part of phases[1]).  phases must hold 4
+ * doubles.  No counterpart in the reference. */
 int curplsh_server_wait_phases(curplsh_server* server, int64_t ticket, double timeout_s, double* latency_s,
                                double* phases);
 int curplsh_server_get_stats(curplsh_server* server, curplsh_server_stats* out);

@@ -46,7 +46,7 @@ def test_python_binding_covers_declarations():
 def test_config_defaults():
     c = cb._Cfg()
     cb._lib.curplsh_bf_config_init(ctypes.byref(c))
-    assert (c.device, c.memory_space, c.precision, c.rerank_factor, c.borrow_device_data) == (0, 0, 0, 4, 0)
+    assert (c.device, c.memory_space, c.precision, c.rerank_factor, c.borrow_device_data) == (0, 0, 0, 0, 0)
     assert c.store_transposed == 0 and c.compute_exact_distances == 0
 
 
