@@ -385,7 +385,7 @@ def run_single(cb, synth, wl, args, world, rank, local, res, peaks, fp8_peak, wi
         "workload": wl, "value": Q * world / (ms / 1e3), "ms_per_step": ms,
         "dtype": FORMS[headline].split("_")[0], "data": info["data"],
         "config": {"workload": wl, "N": n_db, "Q": Q, "d": dim, "k": k, "form": FORMS[headline],
-                   "rerank_factor": {"bf16_rerank": 4, "fp8_rerank": 32}, "l2": info["l2"], "seed": synth.SEEDS[wl],
+                   "kprime": {"bf16_rerank": "4k", "fp8_rerank": "max(4k, 320)", "fp32_exact": "k + 16, rounded up to 32"}, "l2": info["l2"], "seed": synth.SEEDS[wl],
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "recall_at_k": rec, "recall_ok": rec is not None and rec >= 1.0,
         "forms": forms_out,
@@ -645,7 +645,8 @@ def run_serving(cb, synth, args, world, rank, local, res):
                                    "phases_p99_ms": {"queued": float(np.percentile(ph[:, 0], 99)),
                                                      "device": float(np.percentile(ph[:, 1], 99)),
                                                      "retire": float(np.percentile(ph[:, 2], 99)),
-                                                     "gpu_exec": float(np.percentile(ph[:, 3], 99))},
+                                                     "gpu_exec": float(np.percentile(ph[:, 3], 99)),
+                                                     "start_lag": float(np.percentile(ph[:, 4], 99))},
                                    "slowest": [[int(i), sizes[i], round(float(lat[i] * 1e3), 3),
                                                 [round(float(x), 3) for x in ph[i]]] for i in slow],
                                    "achieved_queries_per_s": sum(sizes) / wall, "requests": count,

@@ -579,14 +579,15 @@ class Server:
     def wait_phases(self, ticket: int, timeout: float = -1.0):
         """wait() that also returns the latency's phases (seconds): (latency,
         waiting for a step, step on the device, retiring) on the host clock,
-        and the step's device work itself timed by CUDA events."""
+        the step's device work itself timed by CUDA events, and the time from
+        issue until that work was seen begun."""
         lat = ctypes.c_double(0.0)
-        ph = (ctypes.c_double * 4)()
+        ph = (ctypes.c_double * 5)()
         rc = _lib.curplsh_server_wait_phases(self._h, int(ticket), float(timeout), ctypes.byref(lat), ph)
         if rc != ERR_STATE:
             self._keep.pop(ticket, None)
         _check(rc)
-        return lat.value, ph[0], ph[1], ph[2], ph[3]
+        return lat.value, ph[0], ph[1], ph[2], ph[3], ph[4]
 
     def stats(self) -> dict:
         st = _ServerStats()

@@ -270,20 +270,24 @@ int build_fp8(curplsh_index* ix, cudaStream_t st) {
   return CURPLSH_OK;
 }
 
-// Default rerank factor of a coarse form (a factor <= 0 asks for it): E4M3's
-// coarse error (~2% of a distance) needs a wider candidate margin than BF16's
-// (~0.4%).  On the 10M-row unit-sphere mixture, k' = 4k left 19 of 10,000
-// FP8 queries short of a true neighbour and the coarse-margin check sent 78%
-// of them to the exact form; at k' = 32k none was short and it sent 0.2%.
-int default_rerank_factor(int form) { return form == kFormFP8 ? 32 : 4; }
+// Candidates of a coarse form when no rerank factor is given (<= 0): 4k, and
+// at least 320 for FP8.  E4M3's coarse error (~2% of a distance) needs a
+// wider candidate margin than BF16's (~0.4%): on the 10M-row unit-sphere
+// mixture (k = 10), k' = 40 left 19 of 10,000 FP8 queries short of a true
+// neighbour and the coarse-margin check sent 78% of them to the exact form;
+// at k' = 320 none was short and it sent 0.2%.  A fixed factor of 32 instead
+// would make k' = 3200 at k = 100, where pools that large cost ten times the
+// pass.
+constexpr long long kFP8MinCandidates = 320;
 
 int kprime_for(int form, int k, int rerank_factor, int64_t n) {
   long long kp;
-  if (rerank_factor <= 0) rerank_factor = default_rerank_factor(form);
+  long long want = (long long)(rerank_factor > 0 ? rerank_factor : 4) * k;
+  if (rerank_factor <= 0 && form == kFormFP8) want = std::max(want, kFP8MinCandidates);
   if (form == kFormExact)
     kp = round_up(k + 16, 32);
   else
-    kp = round_up(std::max<long long>((long long)rerank_factor * k, k + 16), 32);
+    kp = round_up(std::max<long long>(want, k + 16), 32);
   kp = std::min<long long>(kp, 4096);
   kp = std::max<long long>(kp, k);
   kp = std::min<long long>(kp, n);
@@ -828,7 +832,7 @@ void curplsh_bf_config_init(curplsh_bf_config* cfg) {
   cfg->device = 0;
   cfg->memory_space = CURPLSH_MEMORY_DEVICE;
   cfg->precision = CURPLSH_PRECISION_FP32_EXACT;
-  cfg->rerank_factor = 0;  // per form: 4 (BF16), 32 (FP8)
+  cfg->rerank_factor = 0;  // the form's default: k' = 4k (FP8: at least 320)
 }
 
 const char* curplsh_last_error(void) { return g_last_error.c_str(); }

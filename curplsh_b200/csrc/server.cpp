@@ -81,7 +81,7 @@ struct Request {
   bool q_dev = false, o_dev = false;
   // host clock: submitted, issued in a step, the step's completion callback
   // ran, results visible to wait()
-  double t_submit = 0, t_issue = 0, t_gpu = 0, t_done = 0;
+  double t_submit = 0, t_issue = 0, t_begin = 0, t_gpu = 0, t_done = 0;
   double gpu_exec = 0;  // seconds between the step's first and last work on its stream (CUDA events)
   int state = kPending;
   int err = CURPLSH_OK;
@@ -105,8 +105,8 @@ struct Step {
   MultiPlan plan;
   // host-output copies to do at completion: (ticket, pinned offset)
   std::vector<std::pair<int64_t, size_t>> host_out;
-  std::atomic<bool> finished{false};
-  double t_gpu_done = 0;  // host clock when the completion callback ran
+  double t_begin_seen = 0;  // host clock when the scheduler first saw the step's work begun
+  double t_gpu_done = 0;    // host clock when the scheduler saw the step's work complete
 };
 
 }  // namespace
@@ -133,17 +133,14 @@ struct curplsh_server {
 
 namespace {
 
-// Queued behind each step.  It takes no lock (a host function that blocks
-// would stall its stream, and a thread holding the lock may be waiting for
-// the device, e.g. inside cudaFree): it sets the flag and wakes the
-// scheduler, whose wait also times out after a short interval in case this
-// wake-up fell between its check and its wait.
-void CUDART_CB on_step_done(void* p) {
-  Step* s = static_cast<Step*>(p);
-  s->t_gpu_done = now_s();
-  s->finished.store(true);
-  s->srv->cv_work.notify_one();
-}
+// Queued behind each step as a wake-up hint only: the scheduler decides that
+// a step is complete by querying the CUDA event recorded after its last copy
+// (host functions run on a driver thread that was seen to run them tens of
+// milliseconds after the work, at low load), and polls every 200 us while
+// steps are in flight.  It takes no lock (a host function that blocks would
+// stall its stream) and touches nothing but the server, which outlives it
+// (destroy synchronises every slot stream before freeing the server).
+void CUDART_CB on_step_done(void* p) { static_cast<curplsh_server*>(p)->cv_work.notify_one(); }
 
 // Pinned staging of one slot: [queries][outputs][status word]; every request
 // rounds its pieces up to 256 bytes.
@@ -201,6 +198,7 @@ void finish_step(curplsh_server* s, Step& st) {
     Request& r = s->reqs[tk];
     r.t_done = t;
     r.t_gpu = st.t_gpu_done;
+    r.t_begin = st.t_begin_seen;
     r.gpu_exec = exec_ms * 1e-3;
     if (status) {
       r.state = kFailed;
@@ -325,7 +323,7 @@ bool issue_step(curplsh_server* s, std::unique_lock<std::mutex>& lk) {
     e = cudaMemcpyAsync(slot.pinned + slot.pinned_bytes - 256, st->plan.status(), sizeof(uint32_t),
                         cudaMemcpyDeviceToHost, slot.st);
   if (!rc && e == cudaSuccess) e = cudaEventRecord(slot.ev_end, slot.st);
-  if (!rc && e == cudaSuccess) e = cudaLaunchHostFunc(slot.st, on_step_done, st.get());
+  if (!rc && e == cudaSuccess) e = cudaLaunchHostFunc(slot.st, on_step_done, s);
   if (rc || e != cudaSuccess) {
     if (e != cudaSuccess) {
       cudaGetLastError();
@@ -364,10 +362,19 @@ void scheduler(curplsh_server* s) {
   std::unique_lock<std::mutex> lk(s->mu);
   for (;;) {
     bool progressed = false;
-    // retire finished steps (oldest first keeps FIFO completion per slot)
+    // retire completed steps (their end event has fired; oldest first keeps
+    // FIFO completion per slot)
+    const double t_poll = now_s();
     for (size_t i = 0; i < s->inflight.size();) {
-      if (s->inflight[i]->finished) {
-        finish_step(s, *s->inflight[i]);
+      Step& stp = *s->inflight[i];
+      const Slot& sl = s->slots[stp.slot];
+      if (stp.t_begin_seen == 0 && cudaEventQuery(sl.ev_begin) == cudaSuccess) stp.t_begin_seen = t_poll;
+      const cudaError_t q = cudaEventQuery(sl.ev_end);
+      if (q != cudaErrorNotReady) {
+        if (q != cudaSuccess) cudaGetLastError();  // an error: finish_step reports the status word
+        stp.t_gpu_done = t_poll;
+        if (stp.t_begin_seen == 0) stp.t_begin_seen = t_poll;
+        finish_step(s, stp);
         s->inflight.erase(s->inflight.begin() + (long)i);
         progressed = true;
       } else {
@@ -538,6 +545,7 @@ int curplsh_server_wait_phases(curplsh_server* s, int64_t ticket, double timeout
     phases[1] = ran ? r.t_gpu - r.t_issue : 0.0;                                 // step issued -> GPU done
     phases[2] = ran ? r.t_done - r.t_gpu : 0.0;                                  // GPU done -> visible
     phases[3] = ran ? r.gpu_exec : 0.0;  // the step's device work itself (CUDA events, inside phases[1])
+    phases[4] = ran ? r.t_begin - r.t_issue : 0.0;  // issue -> its first work seen begun (inside phases[1])
   }
   if (r.state == kFailed) return fail(r.err ? r.err : CURPLSH_ERR_DEVICE, "%s", r.msg.c_str());
   return CURPLSH_OK;

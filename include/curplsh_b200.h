@@ -60,8 +60,8 @@ typedef struct curplsh_bf_config {
   int32_t compute_exact_distances; /* IndexBFConfig::computeExactDistances: IndexBF::search always
                                       returns exact squared distances (src/index_bf.cpp:68-69), so is this */
   int32_t precision;               /* CURPLSH_PRECISION_* default for search */
-  int32_t rerank_factor;           /* k' = rerank_factor * k for the BF16/FP8 forms; 0 (default): 4 for
-                                      BF16, 32 for FP8 (E4M3's coarse error needs the wider margin) */
+  int32_t rerank_factor;           /* k' = rerank_factor * k for the BF16/FP8 forms; 0 (default): k' = 4k,
+                                      and at least 320 for FP8 (E4M3's coarse error needs the margin) */
   int32_t borrow_device_data;      /* 1: add() of device memory keeps a reference to the caller's FP32
                                       rows (the reference's aliasing, include/device_tensor.h:97-103);
                                       0 (default): the index copies them */
@@ -246,10 +246,12 @@ int curplsh_server_submit(curplsh_server* server, int64_t num, const float* quer
  * can be waited for once. */
 int curplsh_server_wait(curplsh_server* server, int64_t ticket, double timeout_s, double* latency_s);
 /* curplsh_server_wait that also splits the latency (host clock) into phases[0..2]: waiting for a
- * step (submit to issue), the step on the device (issue to its completion callback), and
- * retiring (callback to the results being visible to wait); phases[3] is the step's device work
- * itself, timed by CUDA events around it on its stream (part of phases[1]).  phases must hold 4
- * doubles.  No counterpart in the reference. */
+ * step (submit to issue), the step on the device (issue until the scheduler sees its end event
+ * complete), and retiring (until the results are visible to wait); phases[3] is the step's device
+ * work itself, timed by CUDA events around it on its stream, and phases[4] the time from issue
+ * until its begin event was seen complete (both part of phases[1]; the scheduler looks every
+ * 200 us while steps are in flight).  phases must hold 5 doubles.  No counterpart in the
+ * reference. */
 int curplsh_server_wait_phases(curplsh_server* server, int64_t ticket, double timeout_s, double* latency_s,
                                double* phases);
 int curplsh_server_get_stats(curplsh_server* server, curplsh_server_stats* out);

@@ -60,7 +60,7 @@ def test_estimate_matches_plain_search(cb, res, precision, k):
     centers = rng.normal(0.0, 4.0, (512, D))
     base = mixture(rng, N, centers)
     queries = mixture(rng, NQ, centers)
-    ix = cb.IndexBF(res, D, cb.IndexBFConfig(precision=precision))
+    ix = cb.IndexBF(res, D, cb.IndexBFConfig(precision=precision, rerankFactor=4))
     ix.add(N, base)
     rows, step, r = ix.estimate_plan(NQ, k, precision)
     assert rows > 0 and rows % 256 == 0 and step >= 10 and 1 <= r, (rows, step, r)
@@ -93,7 +93,7 @@ def test_estimate_failure_is_searched_again(cb, res, precision, k):
     estimate fails and it must be searched again; queries of the far cluster
     keep theirs."""
     rng = np.random.default_rng(23 + precision)
-    ix = cb.IndexBF(res, D, cb.IndexBFConfig(precision=precision))
+    ix = cb.IndexBF(res, D, cb.IndexBFConfig(precision=precision, rerankFactor=4))
     ix.add(N, rng.normal(0.0, 1.0, (N, D)).astype(np.float32))
     rows, step, r = ix.estimate_plan(NQ, k, precision)
     assert rows > 0
