@@ -270,19 +270,26 @@ int build_fp8(curplsh_index* ix, cudaStream_t st) {
   return CURPLSH_OK;
 }
 
-// Candidates of a coarse form when no rerank factor is given (<= 0): 4k, and
-// at least 320 for FP8.  E4M3's coarse error (~2% of a distance) needs a
-// wider candidate margin than BF16's (~0.4%): on the 10M-row unit-sphere
-// mixture (k = 10), k' = 40 left 19 of 10,000 FP8 queries short of a true
-// neighbour and the coarse-margin check sent 78% of them to the exact form;
-// at k' = 320 none was short and it sent 0.2%.  A fixed factor of 32 instead
+// Candidates of a coarse form when no rerank factor is given (<= 0).
+// BF16: 2k when the search is verified by the coarse-margin check (a query it
+// lists is searched again exactly), else 4k.  On the integer mixture (N = 10^6,
+// k = 100), 2^20 uniform rows and two BF16-valued sets, k' = 2k left no query
+// short of a true neighbour and the check listed none; k' = k listed 1.7% of
+// the uniform queries.  Unverified searches (batch graph, serving loop,
+// allocation-free entry) keep the wider 4k margin.
+// FP8: 4k and at least 320, verified or not.  E4M3's coarse error (~2% of a
+// distance) needs a wider margin than BF16's (~0.4%): on the 10M-row
+// unit-sphere mixture (k = 10), k' = 40 left 19 of 10,000 FP8 queries short of
+// a true neighbour and the check sent 78% of them to the exact form; at
+// k' = 320 none was short and it sent 0.2%.  A fixed factor of 32 instead
 // would make k' = 3200 at k = 100, where pools that large cost ten times the
 // pass.
 constexpr long long kFP8MinCandidates = 320;
 
-int kprime_for(int form, int k, int rerank_factor, int64_t n) {
+int kprime_for(int form, int k, int rerank_factor, int64_t n, bool checked) {
   long long kp;
-  long long want = (long long)(rerank_factor > 0 ? rerank_factor : 4) * k;
+  const int dflt = (form == kFormBF16 && checked) ? 2 : 4;
+  long long want = (long long)(rerank_factor > 0 ? rerank_factor : dflt) * k;
   if (rerank_factor <= 0 && form == kFormFP8) want = std::max(want, kFP8MinCandidates);
   if (form == kFormExact)
     kp = round_up(k + 16, 32);
@@ -420,7 +427,7 @@ bool coarse_check_applies(const curplsh_index* ix, int form, int kp, bool enable
 SearchShape search_shape(const curplsh_index* ix, int nq, int k, int form, int rerank_factor, bool allow_est,
                          bool coarse_on) {
   SearchShape sh;
-  sh.kp = kprime_for(form, k, rerank_factor, ix->n);
+  sh.kp = kprime_for(form, k, rerank_factor, ix->n, coarse_on);
   const TuneParams tp = tune_lookup(form, ix->dim, k, nq);
   sh.P = pool_capacity(sh.kp, tp.headroom);
   plan_fused(nq, (int)ix->n, ix->dres->num_sms, &sh.plan, default_split_q4(tp, sh.P));
@@ -681,12 +688,13 @@ int do_search(curplsh_index* ix, int64_t num, const float* queries, int k, int p
   // A search that starts from an estimated bound checks it on the host (a
   // failed query is searched again), so it always returns synchronised.  The
   // switch is read once here: planning and the check below agree.
-  const int kp = ix->n > 0 ? kprime_for(form, k, rf, ix->n) : 0;
-  const bool est = g_bound_estimate.load(std::memory_order_relaxed) && ix->n > 0 &&
-                   plan_estimate(nq, ix->n, kp, ix->dres->num_sms).on;
   // Likewise the coarse-margin check of the BF16/FP8 forms: a query it lists
   // is searched again in the exact form before the call returns.
-  const bool coarse = coarse_check_applies(ix, form, kp, g_coarse_check.load(std::memory_order_relaxed) != 0);
+  const bool coarse_on = g_coarse_check.load(std::memory_order_relaxed) != 0;
+  const int kp = ix->n > 0 ? kprime_for(form, k, rf, ix->n, coarse_on) : 0;
+  const bool est = g_bound_estimate.load(std::memory_order_relaxed) && ix->n > 0 &&
+                   plan_estimate(nq, ix->n, kp, ix->dres->num_sms).on;
+  const bool coarse = coarse_check_applies(ix, form, kp, coarse_on);
   const bool sync = force_sync || est || coarse || !(q_dev && i_dev && d_dev);
 
   auto& slot = ix->ws[st];
@@ -818,7 +826,9 @@ int index_prepare_form(curplsh_index* ix, int form, IndexView* v) {
   v->xs = ix->xs;
   return CURPLSH_OK;
 }
-int search_kprime(int form, int k, int rerank_factor, long long n) { return kprime_for(form, k, rerank_factor, n); }
+int search_kprime(int form, int k, int rerank_factor, long long n) {
+  return kprime_for(form, k, rerank_factor, n, false);
+}
 int search_pool_capacity(int kprime, int headroom) { return pool_capacity(kprime, headroom); }
 int record_error(int code, const char* msg) { return set_error(code, "%s", msg); }
 }  // namespace curplsh_b200
@@ -1143,7 +1153,8 @@ int curplsh_index_estimate_plan(curplsh_index* ix, int64_t num, int k, int preci
   *step = 1;
   *rank = 0;
   if (ix->n == 0 || !g_bound_estimate.load(std::memory_order_relaxed)) return CURPLSH_OK;
-  const EstimatePlan e = plan_estimate((int)num, ix->n, kprime_for(form, k, rf, ix->n), ix->dres->num_sms);
+  const bool coarse_on = g_coarse_check.load(std::memory_order_relaxed) != 0;
+  const EstimatePlan e = plan_estimate((int)num, ix->n, kprime_for(form, k, rf, ix->n, coarse_on), ix->dres->num_sms);
   if (e.on) {
     *sample_rows = e.rows;
     *step = e.step;

@@ -258,22 +258,35 @@ __device__ __forceinline__ float thr_from(float dstar, float qn) {
 #define STAT_FLUSH(slot, acc)
 #endif
 
-// 1: survivor mask bits are built with set.le (all ones or zero) and one
-// lop3 that ANDs in the bit and ORs it into the partial mask (two
-// instructions a column); 0: with a compare, a select and an or.
-#ifndef CURPLSH_SET_MASKS
-#define CURPLSH_SET_MASKS 0
-#endif
-__device__ __forceinline__ uint32_t set_le_f32(float a, float b) {
+// Survivor masks from sign bits.  t = thr - d is formed two columns at a time
+// by one packed FMA (d * -1 + thr: exact product, one rounding); a column
+// survives iff t >= 0, and rounding never changes the sign of a difference
+// (equal values give +0), so the test is exactly d <= thr.  The sign bits
+// enter the mask by funnel shifts, four consecutive columns per chain, so bit j
+// belongs to column j.  Two instructions of 64 lanes' worth per two columns
+// against three ALU instructions per column for compare, select and or.
+// (acc << 1) | (t >> 31)
+__device__ __forceinline__ uint32_t shl1_sign(uint32_t acc, uint32_t t) {
   uint32_t r;
-  asm("set.le.u32.f32 %0, %1, %2;" : "=r"(r) : "f"(a), "f"(b));
+  asm("shf.l.wrap.b32 %0, %1, %2, 1;" : "=r"(r) : "r"(t), "r"(acc));
   return r;
 }
-// (m & bit) | acc
-__device__ __forceinline__ uint32_t or_masked(uint32_t acc, uint32_t m, uint32_t bit) {
-  uint32_t r;
-  asm("lop3.b32 %0, %1, %2, %3, 0xEA;" : "=r"(r) : "r"(m), "r"(bit), "r"(acc));
-  return r;
+// bit j set iff dv[j] <= thr
+__device__ __forceinline__ uint32_t survive_mask32(const float (&dv)[32], float thr) {
+  float t[32];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) fma2_f32(t[2 * i], t[2 * i + 1], dv[2 * i], dv[2 * i + 1], -1.f, -1.f, thr, thr);
+  uint32_t c[8];
+#pragma unroll
+  for (int p = 0; p < 8; ++p) {
+    uint32_t a = __float_as_uint(t[4 * p + 3]) >> 31;
+#pragma unroll
+    for (int i = 2; i >= 0; --i) a = shl1_sign(a, __float_as_uint(t[4 * p + i]));
+    c[p] = a;  // bit i = sign of t[4p + i]
+  }
+  const uint32_t lo = (((c[3] << 4) | c[2]) << 8) | ((c[1] << 4) | c[0]);
+  const uint32_t hi = (((c[7] << 4) | c[6]) << 8) | ((c[5] << 4) | c[4]);
+  return ~((hi << 16) | lo);
 }
 
 // v[j] for a runtime j in [0, 32) without local memory: a 5-level select tree.
@@ -689,23 +702,9 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
             bmin = fminf(bmin, mm[0]);
             continue;
           }
-          // survivor masks, each OR-combined in eight independent partial masks
-          uint32_t ma = 0u, mb = 0u;
-          {
-            uint32_t pa[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u}, pb[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
-#pragma unroll
-            for (int j = 0; j < 32; ++j) {
-#if CURPLSH_SET_MASKS
-              pa[j & 7] = or_masked(pa[j & 7], set_le_f32(da[j], thr), 1u << j);
-              pb[j & 7] = or_masked(pb[j & 7], set_le_f32(db[j], thr), 1u << j);
-#else
-              pa[j & 7] |= (da[j] <= thr ? 1u : 0u) << j;
-              pb[j & 7] |= (db[j] <= thr ? 1u : 0u) << j;
-#endif
-            }
-            ma = ((pa[0] | pa[1]) | (pa[2] | pa[3])) | ((pa[4] | pa[5]) | (pa[6] | pa[7]));
-            mb = ((pb[0] | pb[1]) | (pb[2] | pb[3])) | ((pb[4] | pb[5]) | (pb[6] | pb[7]));
-          }
+          // survivor masks: bit j of ma / mb for column j of da / db
+          uint32_t ma = survive_mask32(da, thr);
+          uint32_t mb = survive_mask32(db, thr);
           if (!valid) ma = mb = 0u;
           // database rows beyond nb (padding of the last tile) never survive
           if (col0 + 64 > p.nb) {

@@ -20,7 +20,8 @@ struct IndexBFConfig : public IndexConfig {
   bool computeExactDistances;
   /// coarse form: CURPLSH_PRECISION_FP32_EXACT / _BF16_RERANK / _FP8_RERANK
   int precision;
-  /// k' = rerankFactor * k candidates for the BF16 / FP8 forms (0: 4k, and at least 320 for FP8)
+  /// k' = rerankFactor * k candidates for the BF16 / FP8 forms (0: the form's default -- BF16 2k
+  /// when the coarse-margin check is on, else 4k; FP8 4k and at least 320)
   int rerankFactor;
   /// keep a reference to device rows passed to add() instead of copying them
   bool borrowDeviceData;
