@@ -258,24 +258,31 @@ __device__ __forceinline__ float thr_from(float dstar, float qn) {
 #define STAT_FLUSH(slot, acc)
 #endif
 
-// Survivor masks from sign bits.  t = thr - d is formed two columns at a time
-// by one packed FMA (d * -1 + thr: exact product, one rounding); a column
-// survives iff t >= 0, and rounding never changes the sign of a difference
-// (equal values give +0), so the test is exactly d <= thr.  The sign bits
-// enter the mask by funnel shifts, four consecutive columns per chain, so bit j
-// belongs to column j.  Two instructions of 64 lanes' worth per two columns
-// against three ALU instructions per column for compare, select and or.
+// Survivor masks from sign bits.  With u = the float just above thr, a column
+// survives iff d < u, i.e. d <= thr.  t = d - u is formed two columns at a time
+// by one packed FMA (d * 1 - u: exact product, one rounding), and its sign bit
+// is exactly the test: rounding never changes the sign of a nonzero difference,
+// d == u gives +0, and a NaN distance gives a NaN with the sign clear, so it
+// never survives, as with a compare.  The sign bits enter the mask by funnel
+// shifts, four consecutive columns per chain, so bit j belongs to column j: a
+// packed FMA per two columns and a shift per column, against a compare, a
+// select and an or per column.
+__device__ __forceinline__ float next_above(float x) {
+  const uint32_t u = __float_as_uint(x);
+  if (u == 0x80000000u) return __uint_as_float(1u);  // -0: the smallest positive subnormal
+  return __uint_as_float((int32_t)u >= 0 ? u + 1u : u - 1u);
+}
 // (acc << 1) | (t >> 31)
 __device__ __forceinline__ uint32_t shl1_sign(uint32_t acc, uint32_t t) {
   uint32_t r;
   asm("shf.l.wrap.b32 %0, %1, %2, 1;" : "=r"(r) : "r"(t), "r"(acc));
   return r;
 }
-// bit j set iff dv[j] <= thr
-__device__ __forceinline__ uint32_t survive_mask32(const float (&dv)[32], float thr) {
+// bit j set iff dv[j] < u (u = next_above(thr): dv[j] <= thr)
+__device__ __forceinline__ uint32_t survive_mask32(const float (&dv)[32], float u) {
   float t[32];
 #pragma unroll
-  for (int i = 0; i < 16; ++i) fma2_f32(t[2 * i], t[2 * i + 1], dv[2 * i], dv[2 * i + 1], -1.f, -1.f, thr, thr);
+  for (int i = 0; i < 16; ++i) fma2_f32(t[2 * i], t[2 * i + 1], dv[2 * i], dv[2 * i + 1], 1.f, 1.f, -u, -u);
   uint32_t c[8];
 #pragma unroll
   for (int p = 0; p < 8; ++p) {
@@ -286,7 +293,46 @@ __device__ __forceinline__ uint32_t survive_mask32(const float (&dv)[32], float 
   }
   const uint32_t lo = (((c[3] << 4) | c[2]) << 8) | ((c[1] << 4) | c[0]);
   const uint32_t hi = (((c[7] << 4) | c[6]) << 8) | ((c[5] << 4) | c[4]);
-  return ~((hi << 16) | lo);
+  return (hi << 16) | lo;
+}
+
+// bit j set iff dv[j] <= thr, by compare, select and or: eight independent
+// partial masks
+__device__ __forceinline__ uint32_t survive_mask32_cmp(const float (&dv)[32], float thr) {
+  uint32_t pa[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+#pragma unroll
+  for (int j = 0; j < 32; ++j) pa[j & 7] |= (dv[j] <= thr ? 1u : 0u) << j;
+  return ((pa[0] | pa[1]) | (pa[2] | pa[3])) | ((pa[4] | pa[5]) | (pa[6] | pa[7]));
+}
+// 1: the FP32-exact form builds its masks by compare (survive_mask32_cmp).
+#ifndef CURPLSH_EXACT_CMP_MASKS
+#define CURPLSH_EXACT_CMP_MASKS 0
+#endif
+
+// 1: survivors are taken without branches (every lane of a warp on the
+// survivor path reserves pool slots and runs the select trees).
+#ifndef CURPLSH_TAKE_BRANCHFREE
+#define CURPLSH_TAKE_BRANCHFREE 0
+#endif
+
+// 1: a chunk's masks are built only when some lane's smallest distance of the
+// 64 columns (a three-input min tree, 32 instructions) passes.
+#ifndef CURPLSH_MIN_FIRST
+#define CURPLSH_MIN_FIRST 0
+#endif
+__device__ __forceinline__ float min64(const float (&a)[32], const float (&b)[32]) {
+  float r[22];
+#pragma unroll
+  for (int i = 0; i < 10; ++i) r[i] = fmin3(a[3 * i], a[3 * i + 1], a[3 * i + 2]);
+  r[10] = fmin3(a[30], a[31], b[0]);
+#pragma unroll
+  for (int i = 0; i < 10; ++i) r[11 + i] = fmin3(b[1 + 3 * i], b[2 + 3 * i], b[3 + 3 * i]);
+  r[21] = b[31];
+  float s[8];
+#pragma unroll
+  for (int i = 0; i < 7; ++i) s[i] = fmin3(r[3 * i], r[3 * i + 1], r[3 * i + 2]);
+  s[7] = r[21];
+  return fminf(fmin3(s[0], s[1], s[2]), fmin3(s[3], s[4], fmin3(s[5], s[6], s[7])));
 }
 
 // v[j] for a runtime j in [0, 32) without local memory: a 5-level select tree.
@@ -613,6 +659,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
         const int tphys = (t - rot + p.num_tiles) % p.num_tiles;  // database tile of position t
         thr = fminf(thr, thr_s[row]);
         if (nb_ob != kOrdInf) thr = fminf(thr, thr_from<Tr::kFolded>(ord2f(nb_ob), qn));
+        const float thr_up = next_above(thr);  // d <= thr  <=>  d < thr_up
         if (valid) nb_ob = ld_relaxed_u32(&p.q_bound[q]);
         // FP8: this half tile's database norms and scales, loaded before the
         // accumulator wait (their latency overlaps it) and staged in the
@@ -702,9 +749,18 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
             bmin = fminf(bmin, mm[0]);
             continue;
           }
+#if CURPLSH_MIN_FIRST
+          if (!__any_sync(0xffffffffu, valid && min64(da, db) < thr_up)) continue;
+#endif
           // survivor masks: bit j of ma / mb for column j of da / db
-          uint32_t ma = survive_mask32(da, thr);
-          uint32_t mb = survive_mask32(db, thr);
+          uint32_t ma, mb;
+          if (CURPLSH_EXACT_CMP_MASKS && Tr::kProducts == 3) {
+            ma = survive_mask32_cmp(da, thr);
+            mb = survive_mask32_cmp(db, thr);
+          } else {
+            ma = survive_mask32(da, thr_up);
+            mb = survive_mask32(db, thr_up);
+          }
           if (!valid) ma = mb = 0u;
           // database rows beyond nb (padding of the last tile) never survive
           if (col0 + 64 > p.nb) {
@@ -726,11 +782,17 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
             // first of each half with a register select tree (no local memory),
             // a second one the same way, and stash only for the rare rest.
             // slots for this lane's survivors of the 64 columns, reserved at once
+#if CURPLSH_TAKE_BRANCHFREE
+            // every lane reserves (most add 0): no branch, so the select trees
+            // below can run while the shared atomic is in flight
+            int n = atomicAdd(&cnt_s[row], __popc(ma) + __popc(mb));
+#else
             int n = 0;
             {
               const int c = __popc(ma) + __popc(mb);
               if (c) n = atomicAdd(&cnt_s[row], c);
             }
+#endif
             if ((ma & mb) == ~0u) {
               // every column survives (a pool with no bound yet): append all
               // 64 keys in column order, no extraction
@@ -755,11 +817,30 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
                 STAT_INC(st_surv, 1);
               }
             };
+#if CURPLSH_TAKE_BRANCHFREE
+            // the first survivor of each half, straight-line (j = -1: none)
+            auto take2 = [&]() {
+              const int ja = __ffs(ma) - 1, jb = __ffs(mb) - 1;
+              const float xa = select32(da, ja & 31), xb = select32(db, jb & 31);
+              ma &= ma - 1u;
+              mb &= mb - 1u;
+              const bool ha = ja >= 0, hb = jb >= 0;
+              if (ha && n < P) pool[n] = make_key(Tr::kFolded ? xa : xa + qn, (uint32_t)(col0 + ja));
+              n += ha ? 1 : 0;
+              if (hb && n < P) pool[n] = make_key(Tr::kFolded ? xb : xb + qn, (uint32_t)(col0 + 32 + jb));
+              n += hb ? 1 : 0;
+              STAT_INC(st_surv, (ha ? 1 : 0) + (hb ? 1 : 0));
+            };
+            take2();
+            if (__any_sync(0xffffffffu, (ma | mb) != 0u)) {
+              take2();
+#else
             take(ma, da, col0);
             take(mb, db, col0 + 32);
             if (__any_sync(0xffffffffu, (ma | mb) != 0u)) {
               take(ma, da, col0);
               take(mb, db, col0 + 32);
+#endif
               if (__any_sync(0xffffffffu, (ma | mb) != 0u)) {
                 float stash[64];
 #pragma unroll
