@@ -304,16 +304,6 @@ __device__ __forceinline__ uint32_t survive_mask32_cmp(const float (&dv)[32], fl
   for (int j = 0; j < 32; ++j) pa[j & 7] |= (dv[j] <= thr ? 1u : 0u) << j;
   return ((pa[0] | pa[1]) | (pa[2] | pa[3])) | ((pa[4] | pa[5]) | (pa[6] | pa[7]));
 }
-// 1: the FP32-exact form builds its masks by compare (survive_mask32_cmp).
-#ifndef CURPLSH_EXACT_CMP_MASKS
-#define CURPLSH_EXACT_CMP_MASKS 0
-#endif
-
-// 1: survivors are taken without branches (every lane of a warp on the
-// survivor path reserves pool slots and runs the select trees).
-#ifndef CURPLSH_TAKE_BRANCHFREE
-#define CURPLSH_TAKE_BRANCHFREE 0
-#endif
 
 // 1: a chunk's masks are built only when some lane's smallest distance of the
 // 64 columns (a three-input min tree, 32 instructions) passes.
@@ -754,7 +744,10 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
 #endif
           // survivor masks: bit j of ma / mb for column j of da / db
           uint32_t ma, mb;
-          if (CURPLSH_EXACT_CMP_MASKS && Tr::kProducts == 3) {
+          // the FP32-exact form keeps compare masks: with three products per
+          // tile it is bound by the tensor pipe, and the packed-FMA masks
+          // measured slower there (10M-row sphere: 70.9 vs 77.0 ms)
+          if (Tr::kProducts == 3) {
             ma = survive_mask32_cmp(da, thr);
             mb = survive_mask32_cmp(db, thr);
           } else {
@@ -781,18 +774,10 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
             // A lane rarely has more than one survivor per 32 columns: take the
             // first of each half with a register select tree (no local memory),
             // a second one the same way, and stash only for the rare rest.
-            // slots for this lane's survivors of the 64 columns, reserved at once
-#if CURPLSH_TAKE_BRANCHFREE
-            // every lane reserves (most add 0): no branch, so the select trees
-            // below can run while the shared atomic is in flight
+            // slots for this lane's survivors of the 64 columns, reserved at
+            // once by every lane (most add 0): no branch, so the select trees
+            // below run while the shared atomic is in flight
             int n = atomicAdd(&cnt_s[row], __popc(ma) + __popc(mb));
-#else
-            int n = 0;
-            {
-              const int c = __popc(ma) + __popc(mb);
-              if (c) n = atomicAdd(&cnt_s[row], c);
-            }
-#endif
             if ((ma & mb) == ~0u) {
               // every column survives (a pool with no bound yet): append all
               // 64 keys in column order, no extraction
@@ -807,17 +792,6 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
               ma = mb = 0u;
               STAT_INC(st_surv, 64);
             }
-            auto take = [&](uint32_t& m, const float (&dv)[32], int c0) {
-              if (m) {
-                const int j = __ffs(m) - 1;
-                m &= m - 1;
-                const float x = select32(dv, j);
-                if (n < P) pool[n] = make_key(Tr::kFolded ? x : x + qn, (uint32_t)(c0 + j));
-                ++n;
-                STAT_INC(st_surv, 1);
-              }
-            };
-#if CURPLSH_TAKE_BRANCHFREE
             // the first survivor of each half, straight-line (j = -1: none)
             auto take2 = [&]() {
               const int ja = __ffs(ma) - 1, jb = __ffs(mb) - 1;
@@ -834,13 +808,6 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
             take2();
             if (__any_sync(0xffffffffu, (ma | mb) != 0u)) {
               take2();
-#else
-            take(ma, da, col0);
-            take(mb, db, col0 + 32);
-            if (__any_sync(0xffffffffu, (ma | mb) != 0u)) {
-              take(ma, da, col0);
-              take(mb, db, col0 + 32);
-#endif
               if (__any_sync(0xffffffffu, (ma | mb) != 0u)) {
                 float stash[64];
 #pragma unroll
