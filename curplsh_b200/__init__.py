@@ -136,6 +136,8 @@ def _load():
         "curplsh_set_coarse_check": (i32, [i32]),
         "curplsh_index_get_coarse_fallback_count": (i32, [vp, ctypes.POINTER(ctypes.c_int64)]),
         "curplsh_get_coarse_check": (i32, [ctypes.POINTER(ctypes.c_int)]),
+        "curplsh_set_cta_pairs": (i32, [i32]),
+        "curplsh_get_cta_pairs": (i32, [ctypes.POINTER(ctypes.c_int)]),
         "curplsh_index_estimate_plan": (i32, [vp, i64, i32, i32, i32, ctypes.POINTER(ctypes.c_int),
                                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
         "curplsh_index_get_fallback_count": (i32, [vp, ctypes.POINTER(ctypes.c_int64)]),
@@ -167,7 +169,8 @@ EXPORTED_SYMBOLS = (
     "curplsh_server_wait", "curplsh_server_wait_phases", "curplsh_server_get_stats", "curplsh_server_destroy", "curplsh_merge_shard_results",
     "curplsh_set_bound_estimate", "curplsh_get_bound_estimate", "curplsh_index_estimate_plan",
     "curplsh_index_get_fallback_count", "curplsh_estimate_plan_shape", "curplsh_set_coarse_check",
-    "curplsh_get_coarse_check", "curplsh_index_get_coarse_fallback_count",
+    "curplsh_get_coarse_check", "curplsh_index_get_coarse_fallback_count", "curplsh_set_cta_pairs",
+    "curplsh_get_cta_pairs",
 )
 
 
@@ -535,6 +538,19 @@ def set_coarse_check(enabled: bool) -> None:
 def get_coarse_check() -> bool:
     v = ctypes.c_int(0)
     _check(_lib.curplsh_get_coarse_check(ctypes.byref(v)))
+    return bool(v.value)
+
+
+def set_cta_pairs(enabled: bool) -> None:
+    """Process-wide switch of CTA pairs: fused passes over >= 4 query blocks run
+    as clusters of two CTAs sharing one 256-row tensor-core MMA (off by default;
+    results do not depend on it)."""
+    _check(_lib.curplsh_set_cta_pairs(1 if enabled else 0))
+
+
+def get_cta_pairs() -> bool:
+    v = ctypes.c_int(0)
+    _check(_lib.curplsh_get_cta_pairs(ctypes.byref(v)))
     return bool(v.value)
 
 

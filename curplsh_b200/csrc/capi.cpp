@@ -432,7 +432,7 @@ SearchShape search_shape(const curplsh_index* ix, int nq, int k, int form, int r
   sh.P = pool_capacity(sh.kp, tp.headroom);
   plan_fused(nq, (int)ix->n, ix->dres->num_sms, &sh.plan, default_split_q4(tp, sh.P));
   sh.nq_pad = round_up(nq, kBM);
-  sh.pool_lists = (size_t)sh.plan.num_qblocks * kBM * sh.plan.units_per_block;
+  sh.pool_lists = (size_t)sh.plan.pool_rows() * sh.plan.units_per_block;
   if (allow_est) sh.est = plan_estimate(nq, ix->n, sh.kp, ix->dres->num_sms);
   sh.coarse = coarse_check_applies(ix, form, sh.kp, coarse_on);
   return sh;
@@ -1137,6 +1137,17 @@ int curplsh_set_coarse_check(int enabled) {
 int curplsh_get_coarse_check(int* enabled) {
   if (!enabled) return set_error(CURPLSH_ERR_INVALID_ARG, "null argument");
   *enabled = g_coarse_check.load(std::memory_order_relaxed);
+  return CURPLSH_OK;
+}
+
+int curplsh_set_cta_pairs(int enabled) {
+  set_cta_pairs(enabled);
+  return CURPLSH_OK;
+}
+
+int curplsh_get_cta_pairs(int* enabled) {
+  if (!enabled) return set_error(CURPLSH_ERR_INVALID_ARG, "null argument");
+  *enabled = get_cta_pairs();
   return CURPLSH_OK;
 }
 

@@ -115,9 +115,9 @@ struct FusedBatch {
   int num_items;
   int form;
   int d;                   // dimension shared by every item of the launch
-  int pad0;
-  long long total_work;    // sum of G_i * T_i
-  long long work_per_cta;  // W
+  int pair;                // 1: clusters of two CTAs, one 256-row MMA over two query blocks
+  long long total_work;    // sum of G_i * T_i (G_i: query groups of 128 << pair rows)
+  long long work_per_cta;  // W, per CTA (per pair when pair = 1)
   uint32_t* status;        // device error word
   unsigned long long* stats;  // per-role cycle counters, written only by builds with CURPLSH_FUSED_STATS
   const int* run_if;       // non-null: every CTA returns at once unless *run_if != 0

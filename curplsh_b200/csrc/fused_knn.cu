@@ -33,6 +33,7 @@
 
 #include "common.cuh"
 #include <algorithm>
+#include <atomic>
 
 #include "fused_knn.h"
 #include "ptx.cuh"
@@ -93,10 +94,15 @@ struct SmemLayout {
   uint32_t hist_off;   // warp-private radix histograms
   uint32_t pool_off;   // per-row candidate pool counts and bounds
   uint32_t total;      // dynamic smem bytes requested (includes 1 KB alignment slack)
+  uint32_t b_chunk;    // bytes of one B part of a K chunk (this CTA's database rows)
+  uint32_t b_tail;     // bytes of the B tail chunk
 };
 
-__host__ __device__ inline SmemLayout make_layout(int form, int d) {
+// pair = 1: this CTA holds half of each 256-row database tile (CTA pairs).
+__host__ __device__ inline SmemLayout make_layout(int form, int d, int pair = 0) {
   SmemLayout L{};
+  L.b_chunk = pair ? kBChunkBytes / 2 : kBChunkBytes;
+  L.b_tail = pair ? kBTailBytes / 2 : kBTailBytes;
   const bool folded = form != kFormFP8;
   const int chunk_elems = folded ? 64 : 128;
   const int a_parts = (form == kFormExact) ? 2 : 1;
@@ -111,7 +117,7 @@ __host__ __device__ inline SmemLayout make_layout(int form, int d) {
   const int nreg = L.nkc - (L.tail_narrow ? 1 : 0);
   const uint32_t a_res = (uint32_t)nreg * a_parts * kAChunkBytes + (L.tail_narrow ? kATailBytes : 0u);
   // a stage = one regular K chunk of the tile; the last one also carries the tail
-  const uint32_t b_stage = (uint32_t)b_parts * kBChunkBytes + (L.tail_narrow ? kBTailBytes : 0u);
+  const uint32_t b_stage = (uint32_t)b_parts * L.b_chunk + (L.tail_narrow ? L.b_tail : 0u);
   if (((a_res + 1023u) & ~1023u) + 2 * b_stage <= budget) {
     L.a_stream = 0;
     L.a_bytes = (a_res + 1023u) & ~1023u;
@@ -139,12 +145,12 @@ __device__ __forceinline__ uint32_t a_res_off(const SmemLayout& L, int kc, int p
 
 // Offsets inside a stage: B parts, then streamed A parts, then the tail (B, A).
 template <int kAP, int kBP>
-__device__ __forceinline__ uint32_t stage_a_off(int part) {
-  return (uint32_t)kBP * kBChunkBytes + (uint32_t)part * kAChunkBytes;
+__device__ __forceinline__ uint32_t stage_a_off(const SmemLayout& L, int part) {
+  return (uint32_t)kBP * L.b_chunk + (uint32_t)part * kAChunkBytes;
 }
 template <int kAP, int kBP>
 __device__ __forceinline__ uint32_t stage_tail_off(const SmemLayout& L) {
-  return (uint32_t)kBP * kBChunkBytes + (L.a_stream ? (uint32_t)kAP * kAChunkBytes : 0u);
+  return (uint32_t)kBP * L.b_chunk + (L.a_stream ? (uint32_t)kAP * kAChunkBytes : 0u);
 }
 
 // ------------------------------------------------------------------ schedule
@@ -165,11 +171,15 @@ struct FusedArgs {
 // u_ord numbers the units of one query block: the number of cuts (CTA range
 // starts and multiples of L) in (0, t0].  A position that is both kinds of
 // cut leaves one ordinal unused (`gap`): that unit writes zero counts for it.
+// With CTA pairs the space counts query groups of two blocks and a range
+// belongs to a pair; each CTA of the pair gets its own block of the group
+// (block = 2 * group + rank) and the same tiles.
 struct UnitWalk {
   long long pos, end, W;
-  int ii;
-  __device__ UnitWalk(int cta, const FusedBatch& B) : W(B.work_per_cta), ii(0) {
-    pos = (long long)cta * W;
+  int ii, shift, rank;
+  __device__ UnitWalk(int cta, const FusedBatch& B, uint32_t cta_rank)
+      : W(B.work_per_cta), ii(0), shift(B.pair), rank((int)cta_rank) {
+    pos = (long long)(cta >> shift) * W;
     end = pos + W < B.total_work ? pos + W : B.total_work;
   }
   template <int MAXI>
@@ -201,17 +211,21 @@ struct UnitWalk {
       rot = first < T ? (int)first : 0;
     }
     item = ii;
+    qb = (qb << shift) + rank;
     pos += len;
     return true;
   }
 };
 
 // Bounded wait that also gives up as soon as another role has aborted.
-__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
-  if (mbar_try_wait(bar, parity)) return true;
+// `cl`: the arrivals come from the other CTA of a pair (acquire at cluster scope).
+__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                              bool cl = false) {
+  auto poll = [&]() { return cl ? mbar_try_wait_cluster(bar, parity) : mbar_try_wait(bar, parity); };
+  if (poll()) return true;
   const uint64_t t0 = globaltimer_ns();
   for (uint32_t i = 0; i < kWaitPollLimit; ++i) {
-    if (mbar_try_wait(bar, parity)) return true;
+    if (poll()) return true;
     if ((i & 255u) == 255u) {
       if (*abort_flag) return false;
       if (globaltimer_ns() - t0 > kWaitTimeoutNs) return false;
@@ -353,8 +367,13 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
   if (B.run_if && *B.run_if == 0) return;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const SmemLayout L = make_layout(FORM, B.d);
+  const SmemLayout L = make_layout(FORM, B.d, B.pair);
   const int S = L.stages;
+  // CTA pairs: rank 0 issues the MMAs and owns the barriers the pair's loads
+  // complete on; each CTA loads and filters its own query block
+  const bool pair = B.pair != 0;
+  const uint32_t rank = pair ? cluster_ctarank() : 0u;
+  const bool issuer = rank == 0;
 
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.bar_off);
   uint64_t* full = bars;            // [8]
@@ -381,7 +400,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
     mbar_init(a_empty, 1);
     for (int s = 0; s < 2; ++s) {
       mbar_init(&acc_full[s], 1);
-      mbar_init(&acc_empty[s], kEpiWarps);
+      mbar_init(&acc_empty[s], pair ? 2 * kEpiWarps : kEpiWarps);  // both CTAs' epilogue warps
     }
     mbar_init(drain, 1);
     *abort_flag = 0;
@@ -389,11 +408,21 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
     fence_proxy_async_smem();
   }
   if (warp == 1) {
-    tmem_alloc(tmem_slot, 512);
-    tmem_relinquish();
+    if (pair) {
+      tmem_alloc_pair(tmem_slot, 512);
+      tmem_relinquish_pair();
+    } else {
+      tmem_alloc(tmem_slot, 512);
+      tmem_relinquish();
+    }
   }
   tc_fence_before();
-  __syncthreads();
+  // a pair's barriers must be initialised before the other CTA's loads and
+  // arrivals can reach them
+  if (pair)
+    cluster_sync();
+  else
+    __syncthreads();
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
 
@@ -405,7 +434,16 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
     if (lane == 0) {
       const uint64_t pol_db = l2_policy_evict_first();
       const uint64_t pol_q = l2_policy_evict_last();
-      UnitWalk walk(blockIdx.x, B);
+      // a pair's loads complete on rank 0's barriers, which expect both CTAs' bytes
+      auto load = [&](void* dst, const CUtensorMap* m, uint64_t* bar, int c0, int c1, uint64_t pol) {
+        if (pair)
+          tma_load_2d_pair(dst, m, bar, c0, c1, pol);
+        else
+          tma_load_2d(dst, m, bar, c0, c1, pol);
+      };
+      const uint32_t tx_mul = pair ? 2u : 1u;
+      const int half_row = pair ? (int)rank * (kBN / 2) : 0;  // this CTA's rows of a tile
+      UnitWalk walk(blockIdx.x, B, rank);
       int ii, qb, t0, t1, u_ord, rot, unit = 0;
       bool gap;
       uint32_t it = 0;
@@ -426,19 +464,20 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
             break;
           }
           const int nreg = L.nkc - (L.tail_narrow ? 1 : 0);
-          mbar_arrive_expect_tx(a_full, (uint32_t)nreg * Tr::kAParts * kAChunkBytes +
-                                            (L.tail_narrow ? kATailBytes : 0u));
+          if (issuer)
+            mbar_arrive_expect_tx(a_full, tx_mul * ((uint32_t)nreg * Tr::kAParts * kAChunkBytes +
+                                                    (L.tail_narrow ? kATailBytes : 0u)));
           for (int kc = 0; kc < nreg; ++kc)
             for (int part = 0; part < Tr::kAParts; ++part)
-              tma_load_2d(smem + a_res_off(L, kc, part, Tr::kAParts), part ? &tm_q_lo : &tm_q_hi, a_full,
-                          kc * KC, qb * kBM, pol_q);
+              load(smem + a_res_off(L, kc, part, Tr::kAParts), part ? &tm_q_lo : &tm_q_hi, a_full, kc * KC, qb * kBM,
+                   pol_q);
           if (L.tail_narrow)
-            tma_load_2d(smem + a_res_off(L, nreg, 0, Tr::kAParts), &tm_q_tail, a_full, nreg * KC, qb * kBM, pol_q);
+            load(smem + a_res_off(L, nreg, 0, Tr::kAParts), &tm_q_tail, a_full, nreg * KC, qb * kBM, pol_q);
         }
         const int nreg = L.nkc - (L.tail_narrow ? 1 : 0);
         for (int t = t0; t < t1 && ok; ++t) {
           const int T_i = A.items[ii].num_tiles;
-          const int tx_row = ((t - rot + T_i) % T_i) * kBN;  // database tile of position t
+          const int tx_row = ((t - rot + T_i) % T_i) * kBN + half_row;  // database tile of position t
           for (int kc = 0; kc < nreg; ++kc, ++it) {
             const int s = (int)(it % (uint32_t)S);
             STAT_BEGIN(tw);
@@ -450,19 +489,19 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
             STAT_END(tw, st_wait);
             uint8_t* st = smem + L.a_bytes + (uint32_t)s * L.stage_bytes;
             const bool with_tail = L.tail_narrow && kc == nreg - 1;
-            uint32_t tx = (uint32_t)Tr::kBParts * kBChunkBytes + (L.a_stream ? (uint32_t)Tr::kAParts * kAChunkBytes : 0u);
-            if (with_tail) tx += kBTailBytes + (L.a_stream ? kATailBytes : 0u);
-            mbar_arrive_expect_tx(&full[s], tx);
+            uint32_t tx = (uint32_t)Tr::kBParts * L.b_chunk + (L.a_stream ? (uint32_t)Tr::kAParts * kAChunkBytes : 0u);
+            if (with_tail) tx += L.b_tail + (L.a_stream ? kATailBytes : 0u);
+            if (issuer) mbar_arrive_expect_tx(&full[s], tx_mul * tx);
             for (int part = 0; part < Tr::kBParts; ++part)
-              tma_load_2d(st + part * kBChunkBytes, part ? &tm_x_lo : &tm_x_hi, &full[s], kc * KC, tx_row, pol_db);
+              load(st + part * L.b_chunk, part ? &tm_x_lo : &tm_x_hi, &full[s], kc * KC, tx_row, pol_db);
             if (L.a_stream)
               for (int part = 0; part < Tr::kAParts; ++part)
-                tma_load_2d(st + stage_a_off<Tr::kAParts, Tr::kBParts>(part), part ? &tm_q_lo : &tm_q_hi, &full[s],
-                            kc * KC, qb * kBM, pol_q);
+                load(st + stage_a_off<Tr::kAParts, Tr::kBParts>(L, part), part ? &tm_q_lo : &tm_q_hi, &full[s],
+                     kc * KC, qb * kBM, pol_q);
             if (with_tail) {
               uint8_t* tl = st + stage_tail_off<Tr::kAParts, Tr::kBParts>(L);
-              tma_load_2d(tl, &tm_x_tail, &full[s], nreg * KC, tx_row, pol_db);
-              if (L.a_stream) tma_load_2d(tl + kBTailBytes, &tm_q_tail, &full[s], nreg * KC, qb * kBM, pol_q);
+              load(tl, &tm_x_tail, &full[s], nreg * KC, tx_row, pol_db);
+              if (L.a_stream) load(tl + L.b_tail, &tm_q_tail, &full[s], nreg * KC, qb * kBM, pol_q);
             }
           }
         }
@@ -472,10 +511,31 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
     }
   } else if (warp == 1) {
     // ------------------------------------------------------------ MMA issuer
-    if (lane == 0) {
+    if (lane == 0 && issuer) {
       constexpr uint32_t fmt = Tr::kFP8 ? 0u : 1u;  // e4m3 : bf16
-      constexpr uint32_t idesc = make_idesc(fmt, fmt, kBM, kBN);
-      UnitWalk walk(blockIdx.x, B);
+      // a pair's MMA is 256 rows: this CTA's query block, then the partner's
+      const uint32_t idesc = make_idesc(fmt, fmt, pair ? 2 * kBM : kBM, kBN);
+      auto mma = [&](uint32_t d_tmem, uint64_t ad, uint64_t bd, uint32_t acc, bool f8) {
+        if (pair) {
+          if (f8)
+            mma_f8_ss_pair(d_tmem, ad, bd, idesc, acc);
+          else
+            mma_f16_ss_pair(d_tmem, ad, bd, idesc, acc);
+        } else {
+          if (f8)
+            mma_f8_ss(d_tmem, ad, bd, idesc, acc);
+          else
+            mma_f16_ss(d_tmem, ad, bd, idesc, acc);
+        }
+      };
+      // completion goes to the barrier at the same offset in both CTAs of a pair
+      auto commit = [&](uint64_t* bar) {
+        if (pair)
+          mma_commit_pair(bar);
+        else
+          mma_commit(bar);
+      };
+      UnitWalk walk(blockIdx.x, B, rank);
       int ii, qb, t0, t1, u_ord, rot, unit = 0;
       bool gap;
       uint32_t it = 0, tc = 0;
@@ -493,7 +553,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
         for (int t = t0; t < t1 && ok; ++t, ++tc) {
           const uint32_t slot = tc & 1u, use = tc >> 1;
           STAT_BEGIN(ta);
-          if (!wait_or_abort(&acc_empty[slot], (use & 1u) ^ 1u, abort_flag)) {
+          if (!wait_or_abort(&acc_empty[slot], (use & 1u) ^ 1u, abort_flag, pair)) {
             raise_abort(abort_flag, B.status, kErrWaitTimeout);
             ok = false;
             break;
@@ -518,16 +578,13 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
             const int nsteps = rem >= KC ? KC / Tr::kStepElems : (rem + Tr::kStepElems - 1) / Tr::kStepElems;
 #pragma unroll
             for (int pr = 0; pr < Tr::kProducts; ++pr) {
-              const uint32_t a_addr = L.a_stream ? st + stage_a_off<Tr::kAParts, Tr::kBParts>(Tr::a_part(pr))
+              const uint32_t a_addr = L.a_stream ? st + stage_a_off<Tr::kAParts, Tr::kBParts>(L, Tr::a_part(pr))
                                                  : smem_u32(smem + a_res_off(L, kc, Tr::a_part(pr), Tr::kAParts));
-              const uint32_t b_addr = st + Tr::b_part(pr) * kBChunkBytes;
+              const uint32_t b_addr = st + Tr::b_part(pr) * L.b_chunk;
               for (int ks = 0; ks < nsteps; ++ks) {
                 const uint64_t ad = sw128_kmajor_desc(a_addr + ks * 32);
                 const uint64_t bd = sw128_kmajor_desc(b_addr + ks * 32);
-                if (Tr::kFP8)
-                  mma_f8_ss(d_tmem, ad, bd, idesc, accumulate);
-                else
-                  mma_f16_ss(d_tmem, ad, bd, idesc, accumulate);
+                mma(d_tmem, ad, bd, accumulate, Tr::kFP8);
                 accumulate = 1;
               }
             }
@@ -535,22 +592,27 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
               // the 16 norm columns: only hi x hi carries them (lo rows are zero
               // there), so one K step of product 0 with the 32-byte-swizzled tiles
               const uint32_t tl = st + stage_tail_off<Tr::kAParts, Tr::kBParts>(L);
-              const uint32_t a_addr = L.a_stream ? tl + kBTailBytes : smem_u32(smem + a_res_off(L, nreg, 0, Tr::kAParts));
-              mma_f16_ss(d_tmem, sw32_kmajor_desc(a_addr), sw32_kmajor_desc(tl), idesc, 1);
+              const uint32_t a_addr = L.a_stream ? tl + L.b_tail : smem_u32(smem + a_res_off(L, nreg, 0, Tr::kAParts));
+              mma(d_tmem, sw32_kmajor_desc(a_addr), sw32_kmajor_desc(tl), 1, false);
             }
-            mma_commit(&empty[s]);
+            commit(&empty[s]);
           }
           if (!ok) break;
-          mma_commit(&acc_full[slot]);
+          commit(&acc_full[slot]);
         }
-        if (!L.a_stream) mma_commit(a_empty);
+        if (!L.a_stream) commit(a_empty);
         ++unit;
       }
-      // Make sure every issued MMA has retired before TMEM is released.
-      mma_commit(drain);
+      // Make sure every issued MMA has retired before TMEM is released (in
+      // both CTAs of a pair: the commit reaches the partner's drain barrier).
+      commit(drain);
       mbar_wait(drain, 0);
       STAT_FLUSH(kStatMmaWaitFull, st_full);
       STAT_FLUSH(kStatMmaWaitAccEmpty, st_acc);
+    } else if (lane == 0 && pair) {
+      // the partner's MMAs also write this CTA's TMEM and read its shared
+      // memory: wait for its final commit before the teardown
+      mbar_wait(drain, 0);
     }
   } else {
     // ------------------------------------------------------------ epilogue
@@ -570,7 +632,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
     int* cnt_s = reinterpret_cast<int*>(smem + L.pool_off);             // [128] pool counts
     float* thr_s = reinterpret_cast<float*>(smem + L.pool_off) + kBM;   // [128] pool bounds
     const uint32_t lane_base = (uint32_t)(lg * 32) << 16;
-    UnitWalk walk(blockIdx.x, B);
+    UnitWalk walk(blockIdx.x, B, rank);
     int ii, qb, t0, t1, u_ord, rot;
     bool gap;
     uint32_t tc = 0;
@@ -832,7 +894,12 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
               Tr::kFolded ? bmin : bmin + qn;
         tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(&acc_empty[slot]);
+        if (lane == 0) {
+          if (pair)
+            mbar_arrive_remote(&acc_empty[slot], 0);  // the issuer's barrier counts both CTAs
+          else
+            mbar_arrive(&acc_empty[slot]);
+        }
         STAT_END(tfl, st_filter);
         }  // got
         // every S tiles (and at the unit's end) meet the partner warp; leave
@@ -881,10 +948,18 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
   }
 
   tc_fence_before();
-  __syncthreads();
+  // a pair releases its TMEM together, and neither CTA leaves while the
+  // other may still signal its barriers or read its shared memory
+  if (pair)
+    cluster_sync();
+  else
+    __syncthreads();
   if (warp == 1) {
     tc_fence_after();
-    tmem_dealloc(tmem_base, 512);
+    if (pair)
+      tmem_dealloc_pair(tmem_base, 512);
+    else
+      tmem_dealloc(tmem_base, 512);
   }
 #ifdef CURPLSH_FUSED_STATS
   if (threadIdx.x == 0 && B.stats) atomicAdd(&B.stats[kStatCtaCycles], (unsigned long long)(clock64() - t_kernel));
@@ -955,8 +1030,10 @@ cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, 
   a.B.num_items = n;
   a.B.form = FORM;
   a.B.d = specs[0].d;
+  a.B.pair = bp.pair;
   a.B.total_work = bp.total_work;
   a.B.work_per_cta = bp.work_per_cta;
+  const int xrows = kBN >> bp.pair;  // database rows one CTA loads per tile
   a.B.status = status;
   a.B.stats = stats;
   a.B.run_if = run_if;
@@ -990,11 +1067,11 @@ cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, 
     const long long ldq = fp8 ? f.ld8 : f.ld16;
     const int step = it.db_step;
     if (!make_map(&m[kMapQHi], qh, fp8, f.nq_pad, ldq, kBM) ||
-        !make_map(&m[kMapXHi], xh, fp8, f.nb_pad, ldq, kBN, false, step))
+        !make_map(&m[kMapXHi], xh, fp8, f.nb_pad, ldq, xrows, false, step))
       return cudaErrorInvalidValue;
     if (FORM == kFormExact) {
       if (!make_map(&m[kMapQLo], f.ql, false, f.nq_pad, f.ld16, kBM) ||
-          !make_map(&m[kMapXLo], f.xl, false, f.nb_pad, f.ld16, kBN, false, step))
+          !make_map(&m[kMapXLo], f.xl, false, f.nb_pad, f.ld16, xrows, false, step))
         return cudaErrorInvalidValue;
     } else {
       m[kMapQLo] = m[kMapQHi];
@@ -1002,15 +1079,31 @@ cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, 
     }
     if (FORM != kFormFP8) {
       if (!make_map(&m[kMapQTail], f.qh, false, f.nq_pad, f.ld16, kBM, true) ||
-          !make_map(&m[kMapXTail], f.xh, false, f.nb_pad, f.ld16, kBN, true, step))
+          !make_map(&m[kMapXTail], f.xh, false, f.nb_pad, f.ld16, xrows, true, step))
         return cudaErrorInvalidValue;
     } else {
       m[kMapQTail] = m[kMapQHi];
       m[kMapXTail] = m[kMapXHi];
     }
   }
-  fused_knn_kernel<FORM, MAXI, MINIMA><<<bp.grid, kNumThreads, smem, st>>>(a);
-  return cudaGetLastError();
+  if (!bp.pair) {
+    fused_knn_kernel<FORM, MAXI, MINIMA><<<bp.grid, kNumThreads, smem, st>>>(a);
+    return cudaGetLastError();
+  }
+  if (bp.grid % 2) return cudaErrorInvalidValue;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)bp.grid, 1, 1);
+  cfg.blockDim = dim3(kNumThreads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, fused_knn_kernel<FORM, MAXI, MINIMA>, a);
 }
 
 template <int FORM>
@@ -1027,23 +1120,44 @@ cudaError_t launch_form_any(const FusedItemSpec* specs, const FusedItemPlan* pla
 
 }  // namespace
 
+namespace {
+std::atomic<int> g_cta_pairs{0};
+}  // namespace
+
+void set_cta_pairs(int on) { g_cta_pairs.store(on ? 1 : 0, std::memory_order_relaxed); }
+int get_cta_pairs() { return g_cta_pairs.load(std::memory_order_relaxed); }
+
 void plan_fused_batch(const FusedItemSpec* specs, int n, int max_ctas, FusedItemPlan* plans, FusedBatchPlan* out) {
+  // CTA pairs when there are enough query blocks and few groups of two would
+  // be half empty (an item with an odd block count leaves one CTA of its last
+  // group without queries)
+  long long blocks = 0, odd = 0;
+  for (int i = 0; i < n; ++i) {
+    const long long g = specs[i].nb > 0 ? (specs[i].nq + kBM - 1) / kBM : 0;
+    blocks += g;
+    odd += g & 1;
+  }
+  const int pair = (get_cta_pairs() && max_ctas >= 2 && blocks >= 4 && odd * 8 <= blocks) ? 1 : 0;
+  const int rows = kBM << pair;
   long long total = 0;
   for (int i = 0; i < n; ++i) {
     FusedItemPlan& pl = plans[i];
-    pl.num_qblocks = specs[i].nb > 0 ? (specs[i].nq + kBM - 1) / kBM : 0;
+    pl.num_qblocks = specs[i].nb > 0 ? (specs[i].nq + rows - 1) / rows : 0;
     pl.num_tiles = (specs[i].nb + kBN - 1) / kBN;
     pl.split_tiles = specs[i].split_tiles > 0 && specs[i].split_tiles < pl.num_tiles ? specs[i].split_tiles
                                                                                       : std::max(pl.num_tiles, 1);
     pl.work_begin = total;
     total += (long long)pl.num_qblocks * pl.num_tiles;
     pl.work_end = total;
+    pl.pair = pair;
   }
-  long long grid = max_ctas < total ? max_ctas : total;
+  const long long units = max_ctas >> pair;  // CTAs, or pairs of CTAs
+  long long grid = units < total ? units : total;
   if (grid < 1) grid = 1;
+  out->pair = pair;
   out->total_work = total;
   out->work_per_cta = total > 0 ? (total + grid - 1) / grid : 1;
-  out->grid = total > 0 ? (int)((total + out->work_per_cta - 1) / out->work_per_cta) : 0;
+  out->grid = total > 0 ? (int)((total + out->work_per_cta - 1) / out->work_per_cta) << pair : 0;
   const long long W = out->work_per_cta;
   for (int i = 0; i < n; ++i) {
     FusedItemPlan& pl = plans[i];
@@ -1072,6 +1186,7 @@ void plan_fused(int nq, int nb, int num_sms, FusedPlan* out, int split_q4) {
   out->num_tiles = ip.num_tiles;
   out->work_per_cta = bp.work_per_cta;
   out->grid = bp.grid;
+  out->pair = bp.pair;
   out->units_per_block = ip.units_per_block;
   out->split_tiles = ip.split_tiles;
 }
@@ -1102,7 +1217,7 @@ cudaError_t launch_fused_batch(int form, const FusedItemSpec* specs, const Fused
   for (int i = 1; i < n; ++i)
     if (specs[i].d != specs[0].d) return cudaErrorInvalidValue;
   if (bp.grid == 0) return cudaSuccess;
-  const uint32_t smem = make_layout(form, specs[0].d).total;
+  const uint32_t smem = make_layout(form, specs[0].d, bp.pair).total;
   if (smem > 227u * 1024u) return cudaErrorInvalidConfiguration;  // a layout bug, not a caller error
   switch (form) {
     case kFormExact:
@@ -1149,10 +1264,12 @@ cudaError_t launch_fused(const FusedLaunch& f, cudaStream_t st) {
   ip.split_tiles = f.plan.split_tiles > 0 ? f.plan.split_tiles : std::max(f.plan.num_tiles, 1);
   ip.work_begin = 0;
   ip.work_end = (long long)f.plan.num_qblocks * f.plan.num_tiles;
+  ip.pair = f.plan.pair;
   FusedBatchPlan bp;
   bp.total_work = ip.work_end;
   bp.work_per_cta = f.plan.work_per_cta;
   bp.grid = f.plan.grid;
+  bp.pair = f.plan.pair;
   return launch_fused_batch(f.form, &s, &ip, 1, bp, f.status, f.stats, st, f.run_if);
 }
 

@@ -8,12 +8,15 @@
 namespace curplsh_b200 {
 
 struct FusedPlan {
-  int num_qblocks = 0;        // G = ceil(nq / 128)
+  int num_qblocks = 0;        // G = ceil(nq / (128 << pair)): query blocks, or groups of two with CTA pairs
   int num_tiles = 0;          // T = ceil(nb / 256)
   long long work_per_cta = 0; // W
   int grid = 0;               // CTAs launched
   int units_per_block = 0;    // U: max units (pool lists) of one query block
   int split_tiles = 1;        // L: resolved unit length limit
+  int pair = 0;               // 1: clusters of two CTAs share each 256-row MMA (two query blocks)
+  // pool rows of the plan (pools and counts are indexed by query row)
+  long long pool_rows() const { return (long long)num_qblocks * (128LL << pair); }
 };
 
 // Tuned launch parameters for one (form, d, k, Q) bucket (tuning.cpp).
@@ -101,14 +104,19 @@ struct FusedItemSpec {
   float* minima;            // non-null: block-minimum mode (FusedItem::minima)
 };
 struct FusedItemPlan {
-  int num_qblocks, num_tiles, units_per_block;
+  int num_qblocks, num_tiles, units_per_block;  // num_qblocks: groups of 128 << pair query rows
   int split_tiles;  // resolved split length L (>= 1)
   long long work_begin, work_end;
+  int pair;         // the launch's FusedBatchPlan::pair
 };
 struct FusedBatchPlan {
   long long total_work = 0, work_per_cta = 1;
   int grid = 0;
+  int pair = 0;  // 1: clusters of two CTAs; work_per_cta is per pair and grid counts CTAs
 };
+// CTA pairs on (1, default) or off for the plans made after the call.
+void set_cta_pairs(int on);
+int get_cta_pairs();
 // Plans `n` items over at most `max_ctas` CTAs.  Only nq, nb and split_tiles
 // of the specs are read, so pool sizes (which depend on units_per_block) can be computed
 // from the plan before the pools are carved.
@@ -207,6 +215,7 @@ cudaError_t launch_merge_rerank(const MergeLaunch& m, cudaStream_t st);
 constexpr int kMergeMaxItems = 128;
 struct MergeItem {
   int nq, k, kprime, pool_cap, num_tiles, units_per_block;
+  int pair;                // the fused launch ran CTA pairs (query groups of 256 rows)
   int row0;                // first pool row of this item within its fused item
   int split_tiles;         // the fused item's resolved split length L
   long long work_begin;    // the fused item's offset in its launch's flattened work space

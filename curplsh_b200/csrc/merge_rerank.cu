@@ -96,7 +96,13 @@ __device__ uint64_t block_select_bound(Each each, uint32_t keep, uint32_t* hist,
   return ~0ull;
 }
 
-__global__ void __launch_bounds__(kMergeThreads) merge_rerank_kernel(const __grid_constant__ MergeArgs a) {
+// Resident CTAs per SM the register allocation must allow (each query's CTA
+// spends most of its time waiting on gathers, so occupancy hides latency).
+#ifndef CURPLSH_MERGE_MIN_BLOCKS
+#define CURPLSH_MERGE_MIN_BLOCKS 1
+#endif
+__global__ void __launch_bounds__(kMergeThreads, CURPLSH_MERGE_MIN_BLOCKS)
+    merge_rerank_kernel(const __grid_constant__ MergeArgs a) {
   if (a.run_if && *a.run_if == 0) return;  // a conditional re-merge whose check passed
   int lo = 0, hi = a.num_items - 1;  // last item with q_begin <= blockIdx.x
   while (lo < hi) {
@@ -122,14 +128,14 @@ __global__ void __launch_bounds__(kMergeThreads) merge_rerank_kernel(const __gri
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   const int prow = m.row0 + q;  // pool row within the fused item
-  const int qb = prow / kBM, row = prow % kBM;
+  const int qb = prow / (kBM << m.pair);  // query block (group of two with CTA pairs)
   const int T = m.num_tiles, U = m.units_per_block;
   const long long W = m.work_per_cta;
   const long long first = (m.work_begin + (long long)qb * T) / W;
   const long long last = (m.work_begin + (long long)(qb + 1) * T - 1) / W;
   // an empty database has no pools; otherwise one list per unit
   const int nlists = T > 0 ? (int)(last - first + 1 + (T - 1) / m.split_tiles) : 0;
-  const size_t list0 = ((size_t)qb * kBM + row) * U;  // pool-list index of unit 0
+  const size_t list0 = (size_t)prow * U;  // pool-list index of unit 0
   // Final bound of the fused pass on this query's k'-th coarse distance: the
   // smallest k'-th of any pool, or the estimate the pass started from.  When
   // it comes from a pool, every key of the k' smallest has a distance <= it.
@@ -444,6 +450,7 @@ cudaError_t launch_merge_rerank(const MergeLaunch& m, cudaStream_t st) {
   it.pool_cap = m.pool_cap;
   it.num_tiles = m.plan.num_tiles;
   it.units_per_block = m.plan.units_per_block;
+  it.pair = m.plan.pair;
   it.row0 = 0;
   it.split_tiles = m.plan.split_tiles > 0 ? m.plan.split_tiles : 1;
   it.work_begin = 0;

@@ -182,7 +182,7 @@ int MultiPlan::build(const curplsh_batch_item* items, int n, const std::vector<c
     x.o_bounds = o_bounds_ + bcur * sizeof(uint32_t);
     bcur += (size_t)x.nq_pad;
     if (v.n == 0) continue;
-    const size_t lists = (size_t)x.plan.num_qblocks * kBM * x.plan.units_per_block;
+    const size_t lists = (size_t)x.plan.num_qblocks * ((size_t)kBM << x.plan.pair) * x.plan.units_per_block;
     if (x.form != kFormFP8) x.o_qh = take((size_t)x.nq_pad * v.ld16 * 2);
     if (x.form == kFormExact) x.o_ql = take((size_t)x.nq_pad * v.ld16 * 2);
     if (x.form == kFormFP8) x.o_q8 = take((size_t)x.nq_pad * v.ld8);
@@ -364,6 +364,7 @@ int MultiPlan::enqueue(cudaStream_t main, const std::vector<cudaStream_t>* branc
           m.pool_cap = x.P;
           m.num_tiles = v.n > 0 ? x.plan.num_tiles : 0;
           m.units_per_block = v.n > 0 ? x.plan.units_per_block : 1;
+          m.pair = x.plan.pair;
           m.row0 = x.row0[j];
           m.split_tiles = v.n > 0 ? x.plan.split_tiles : 1;
           m.work_begin = x.plan.work_begin;

@@ -153,7 +153,7 @@ int search_noalloc_locked(const IndexView& v, int nq, const float* q, int k, int
   int cap = v.num_sms;
   for (;;) {
     plan_fused(nq, (int)v.n, cap, &plan);
-    const size_t lists = (size_t)plan.num_qblocks * kBM * plan.units_per_block;
+    const size_t lists = (size_t)plan.pool_rows() * plan.units_per_block;
     L = carve(form, nq_pad, v.ld16, v.ld8, lists, P);
     if (L.total <= kNoAllocScratchBytes || cap == 1) break;
     cap = cap * 3 / 4 > 1 ? cap * 3 / 4 : 1;

@@ -324,6 +324,13 @@ int curplsh_index_get_fallback_count(curplsh_index* index, int64_t* count);
  * it returns synchronised even with device buffers.  Process-wide; on (1) by default. */
 int curplsh_set_coarse_check(int enabled);
 int curplsh_get_coarse_check(int* enabled);
+/* CTA pairs (engine-specific, no counterpart in cuRPLSH; off by default): with it on, a fused
+ * pass over at least four 128-query blocks runs as clusters of two CTAs, each pair sharing one
+ * 256-row tensor-core MMA (tcgen05 cta_group::2) over two query blocks, so every database tile
+ * crosses from L2 once per 256 queries instead of once per 128.  Results do not depend on it.
+ * Applies to searches, batches and servers planned after the call.  Process-wide. */
+int curplsh_set_cta_pairs(int enabled);
+int curplsh_get_cta_pairs(int* enabled);
 /* Number of queries this index searched again in the exact form after their coarse margin
  * failed (since creation). */
 int curplsh_index_get_coarse_fallback_count(curplsh_index* index, int64_t* count);
