@@ -357,7 +357,10 @@ __device__ __forceinline__ float select32(const float (&v)[32], int j) {
 // MINIMA selects the block-minimum mode (FusedItem::minima, the sample pass of
 // the bound estimate) at compile time, so the candidate-pool kernel carries
 // none of its code.
-template <int FORM, int MAXI, bool MINIMA = false>
+// PAIR selects the CTA-pair kernel: a kernel that contains cta_group::2
+// instructions can only be launched as clusters of two, so the single-CTA
+// kernel is a separate instance without them.
+template <int FORM, int MAXI, bool MINIMA = false, bool PAIR = false>
 __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_constant__ FusedArgs<MAXI> A) {
   using Tr = FormTraits<FORM>;
   const FusedBatch& B = A.B;
@@ -367,12 +370,13 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
   if (B.run_if && *B.run_if == 0) return;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const SmemLayout L = make_layout(FORM, B.d, B.pair);
+  const SmemLayout L = make_layout(FORM, B.d, PAIR ? 1 : 0);
   const int S = L.stages;
   // CTA pairs: rank 0 issues the MMAs and owns the barriers the pair's loads
   // complete on; each CTA loads and filters its own query block
-  const bool pair = B.pair != 0;
-  const uint32_t rank = pair ? cluster_ctarank() : 0u;
+  constexpr bool pair = PAIR;
+  uint32_t rank = 0u;
+  if constexpr (PAIR) rank = cluster_ctarank();
   const bool issuer = rank == 0;
 
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.bar_off);
@@ -408,7 +412,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
     fence_proxy_async_smem();
   }
   if (warp == 1) {
-    if (pair) {
+    if constexpr (PAIR) {
       tmem_alloc_pair(tmem_slot, 512);
       tmem_relinquish_pair();
     } else {
@@ -419,7 +423,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
   tc_fence_before();
   // a pair's barriers must be initialised before the other CTA's loads and
   // arrivals can reach them
-  if (pair)
+  if constexpr (PAIR)
     cluster_sync();
   else
     __syncthreads();
@@ -436,7 +440,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
       const uint64_t pol_q = l2_policy_evict_last();
       // a pair's loads complete on rank 0's barriers, which expect both CTAs' bytes
       auto load = [&](void* dst, const CUtensorMap* m, uint64_t* bar, int c0, int c1, uint64_t pol) {
-        if (pair)
+        if constexpr (PAIR)
           tma_load_2d_pair(dst, m, bar, c0, c1, pol);
         else
           tma_load_2d(dst, m, bar, c0, c1, pol);
@@ -516,7 +520,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
       // a pair's MMA is 256 rows: this CTA's query block, then the partner's
       const uint32_t idesc = make_idesc(fmt, fmt, pair ? 2 * kBM : kBM, kBN);
       auto mma = [&](uint32_t d_tmem, uint64_t ad, uint64_t bd, uint32_t acc, bool f8) {
-        if (pair) {
+        if constexpr (PAIR) {
           if (f8)
             mma_f8_ss_pair(d_tmem, ad, bd, idesc, acc);
           else
@@ -530,7 +534,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
       };
       // completion goes to the barrier at the same offset in both CTAs of a pair
       auto commit = [&](uint64_t* bar) {
-        if (pair)
+        if constexpr (PAIR)
           mma_commit_pair(bar);
         else
           mma_commit(bar);
@@ -895,7 +899,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
         tc_fence_before();
         __syncwarp();
         if (lane == 0) {
-          if (pair)
+          if constexpr (PAIR)
             mbar_arrive_remote(&acc_empty[slot], 0);  // the issuer's barrier counts both CTAs
           else
             mbar_arrive(&acc_empty[slot]);
@@ -950,13 +954,13 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
   tc_fence_before();
   // a pair releases its TMEM together, and neither CTA leaves while the
   // other may still signal its barriers or read its shared memory
-  if (pair)
+  if constexpr (PAIR)
     cluster_sync();
   else
     __syncthreads();
   if (warp == 1) {
     tc_fence_after();
-    if (pair)
+    if constexpr (PAIR)
       tmem_dealloc_pair(tmem_base, 512);
     else
       tmem_dealloc(tmem_base, 512);
@@ -1005,13 +1009,13 @@ bool make_map(CUtensorMap* m, const void* base, bool fp8, long long rows, long l
 }
 
 // Raises the kernel's dynamic shared memory limit once per device.
-template <int FORM, int MAXI, bool MINIMA = false>
+template <int FORM, int MAXI, bool MINIMA = false, bool PAIR = false>
 cudaError_t ensure_attributes() {
   static bool attr_done[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr_done[dev & 63]) {
-    cudaError_t e = cudaFuncSetAttribute(fused_knn_kernel<FORM, MAXI, MINIMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(fused_knn_kernel<FORM, MAXI, MINIMA, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          227 * 1024);
     if (e != cudaSuccess) return e;
     attr_done[dev & 63] = true;
@@ -1019,11 +1023,11 @@ cudaError_t ensure_attributes() {
   return cudaSuccess;
 }
 
-template <int FORM, int MAXI, bool MINIMA = false>
+template <int FORM, int MAXI, bool MINIMA = false, bool PAIR = false>
 cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, int n, const FusedBatchPlan& bp,
                         uint32_t* status, unsigned long long* stats, uint32_t smem, cudaStream_t st,
                         const int* run_if) {
-  cudaError_t e = ensure_attributes<FORM, MAXI, MINIMA>();
+  cudaError_t e = ensure_attributes<FORM, MAXI, MINIMA, PAIR>();
   if (e != cudaSuccess) return e;
   FusedArgs<MAXI> a;
   memset(&a, 0, sizeof(a));
@@ -1086,8 +1090,8 @@ cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, 
       m[kMapXTail] = m[kMapXHi];
     }
   }
-  if (!bp.pair) {
-    fused_knn_kernel<FORM, MAXI, MINIMA><<<bp.grid, kNumThreads, smem, st>>>(a);
+  if (!PAIR) {
+    fused_knn_kernel<FORM, MAXI, MINIMA, PAIR><<<bp.grid, kNumThreads, smem, st>>>(a);
     return cudaGetLastError();
   }
   if (bp.grid % 2) return cudaErrorInvalidValue;
@@ -1103,7 +1107,7 @@ cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, 
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, fused_knn_kernel<FORM, MAXI, MINIMA>, a);
+  return cudaLaunchKernelEx(&cfg, fused_knn_kernel<FORM, MAXI, MINIMA, PAIR>, a);
 }
 
 template <int FORM>
@@ -1111,11 +1115,15 @@ cudaError_t launch_form_any(const FusedItemSpec* specs, const FusedItemPlan* pla
                             uint32_t* status, unsigned long long* stats, uint32_t smem, cudaStream_t st,
                             const int* run_if) {
   if (n == 1 && specs[0].minima)
-    return launch_form<FORM, 1, true>(specs, plans, n, bp, status, stats, smem, st, run_if);
+    return bp.pair ? launch_form<FORM, 1, true, true>(specs, plans, n, bp, status, stats, smem, st, run_if)
+                   : launch_form<FORM, 1, true>(specs, plans, n, bp, status, stats, smem, st, run_if);
   for (int i = 0; i < n; ++i)
     if (specs[i].minima) return cudaErrorInvalidValue;  // block-minimum mode is single-item
-  if (n == 1) return launch_form<FORM, 1>(specs, plans, n, bp, status, stats, smem, st, run_if);
-  return launch_form<FORM, kFusedMaxItems>(specs, plans, n, bp, status, stats, smem, st, run_if);
+  if (n == 1)
+    return bp.pair ? launch_form<FORM, 1, false, true>(specs, plans, n, bp, status, stats, smem, st, run_if)
+                   : launch_form<FORM, 1>(specs, plans, n, bp, status, stats, smem, st, run_if);
+  return bp.pair ? launch_form<FORM, kFusedMaxItems, false, true>(specs, plans, n, bp, status, stats, smem, st, run_if)
+                 : launch_form<FORM, kFusedMaxItems>(specs, plans, n, bp, status, stats, smem, st, run_if);
 }
 
 }  // namespace
@@ -1198,12 +1206,24 @@ cudaError_t prepare_fused_kernels(int form) {
   switch (form) {
     case kFormExact:
       e = ensure_attributes<kFormExact, 1>();
+      if (e == cudaSuccess) e = ensure_attributes<kFormExact, 1, true>();
+      if (e == cudaSuccess) e = ensure_attributes<kFormExact, 1, false, true>();
+      if (e == cudaSuccess) e = ensure_attributes<kFormExact, 1, true, true>();
+      if (e == cudaSuccess) e = ensure_attributes<kFormExact, kFusedMaxItems, false, true>();
       return e != cudaSuccess ? e : ensure_attributes<kFormExact, kFusedMaxItems>();
     case kFormBF16:
       e = ensure_attributes<kFormBF16, 1>();
+      if (e == cudaSuccess) e = ensure_attributes<kFormBF16, 1, true>();
+      if (e == cudaSuccess) e = ensure_attributes<kFormBF16, 1, false, true>();
+      if (e == cudaSuccess) e = ensure_attributes<kFormBF16, 1, true, true>();
+      if (e == cudaSuccess) e = ensure_attributes<kFormBF16, kFusedMaxItems, false, true>();
       return e != cudaSuccess ? e : ensure_attributes<kFormBF16, kFusedMaxItems>();
     case kFormFP8:
       e = ensure_attributes<kFormFP8, 1>();
+      if (e == cudaSuccess) e = ensure_attributes<kFormFP8, 1, true>();
+      if (e == cudaSuccess) e = ensure_attributes<kFormFP8, 1, false, true>();
+      if (e == cudaSuccess) e = ensure_attributes<kFormFP8, 1, true, true>();
+      if (e == cudaSuccess) e = ensure_attributes<kFormFP8, kFusedMaxItems, false, true>();
       return e != cudaSuccess ? e : ensure_attributes<kFormFP8, kFusedMaxItems>();
     default:
       return cudaErrorInvalidValue;
