@@ -372,7 +372,10 @@ double binomial_tail(int n, double q, int j) {
 // mu = expected sample rows among a query's k' nearest.  A larger sample gives
 // a tighter rank (j / mu falls from ~2.6 at mu = 12 to ~2 at 24) but costs
 // more; the sample pass takes at most a tenth of the full pass's tiles.
-constexpr double kEstimateMuMax = 24.0;
+#ifndef CURPLSH_ESTIMATE_MU
+#define CURPLSH_ESTIMATE_MU 24.0
+#endif
+constexpr double kEstimateMuMax = CURPLSH_ESTIMATE_MU;
 constexpr double kEstimateMuMin = 8.0;
 constexpr double kEstimateFailure = 1e-6;   // per-query failure probability for a uniform sample
 constexpr int kEstimateBlockRows = kHalfN;  // rows per block minimum (one epilogue warp's half tile)
