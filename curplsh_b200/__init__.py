@@ -330,9 +330,10 @@ class IndexBF:
     def search_ex(self, num: int, queries, k: int, indices, distances, precision: int = -1,
                   rerank_factor: int = -1, stream=None) -> None:
         """search with an explicit precision form, rerank factor and stream.  With device
-        buffers the call is asynchronous on `stream`, except when the search uses the
-        sampled bound estimate (large searches; see ``estimate_plan``): it then returns
-        synchronised, after searching again any query whose estimate failed."""
+        buffers the call is asynchronous on `stream`, except when the BF16/FP8 coarse-margin
+        check applies (it then returns synchronised, after searching again in the exact
+        form any query the check lists).  A sampled bound estimate is verified on the
+        stream in the asynchronous case and by the host otherwise."""
         _check(_lib.curplsh_index_search_ex(self._h, int(num), _ptr(queries, np.float32), int(k), int(precision),
                                             int(rerank_factor), _ptr(indices, np.int32, True),
                                             _ptr(distances, np.float32, True), _stream_ptr(stream)))

@@ -226,7 +226,8 @@ struct curplsh_index {
   __nv_bfloat16* xl = nullptr;    // [n_pad x ld16]
   uint8_t* x8 = nullptr;          // [n_pad x ld8]   (built on first FP8 search)
   float* xs = nullptr;            // [n_pad]
-  uint32_t* status = nullptr;     // device words: [0] error status, [1] nonzero if a row is not exactly BF16
+  uint32_t* status = nullptr;     // device words: [0] error status, [1] nonzero if a row is not exactly BF16,
+                                  // [2..3] 64-bit count of queries whose estimate failed in device-checked searches
   bool bf16_exact = false;        // every stored value is exactly a BF16 value (rerank reads xh)
   long long generation = 0;       // bumped whenever the prepared database changes (add, reset)
   cudaEvent_t order_ev = nullptr; // orders default-stream searches after the legacy stream
@@ -373,7 +374,7 @@ double binomial_tail(int n, double q, int j) {
 // a tighter rank (j / mu falls from ~2.6 at mu = 12 to ~2 at 24) but costs
 // more; the sample pass takes at most a tenth of the full pass's tiles.
 #ifndef CURPLSH_ESTIMATE_MU
-#define CURPLSH_ESTIMATE_MU 24.0
+#define CURPLSH_ESTIMATE_MU 12.0
 #endif
 constexpr double kEstimateMuMax = CURPLSH_ESTIMATE_MU;
 constexpr double kEstimateMuMin = 8.0;
@@ -509,9 +510,14 @@ cudaError_t fused_stats_print(const char* label, const FusedLaunch& f, cudaStrea
 // BF16/FP8 forms check their coarse margin; when either applies, *fail_out
 // points at the device list of queries that failed a check ([0] count, then
 // indices), which the caller must search again (else *fail_out is null).
+// With `dev_recheck` (and no coarse check) a failed estimate is handled on the
+// stream instead: when the merge lists any query, the full pass and the merge
+// run again from no bound for the whole batch (rare: the estimate fails with
+// probability ~1e-6 per query), the failures are counted on the device, and
+// *fail_out stays null, so the caller need not synchronise.
 int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form, int rerank_factor, int* out_idx,
                   float* out_dist, cudaStream_t st, char* extra_base, Timing* tm, bool allow_est, bool coarse_on,
-                  int** fail_out) {
+                  int** fail_out, bool dev_recheck) {
   const int d = ix->dim;
   *fail_out = nullptr;
   if (ix->n == 0) {
@@ -618,6 +624,22 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
   m.out_dist = out_dist;
   m.status = ix->status;
   CUDA_TRY(launch_merge_rerank(m, st));
+  if (dev_recheck && m.checks == kCheckEstimate) {
+    CUDA_TRY(launch_fill_u32_if(b.qbound, nq_pad, 0xFFFFFFFFu, b.fail, st));
+    FusedLaunch f2 = f;
+    f2.run_if = b.fail;
+    CUDA_TRY(launch_fused(f2, st));
+    MergeLaunch m2 = m;
+    m2.checks = 0;
+    m2.fail_count = nullptr;
+    m2.coarse_count = nullptr;
+    m2.fail_list = nullptr;
+    m2.run_if = b.fail;
+    CUDA_TRY(launch_merge_rerank(m2, st));
+    CUDA_TRY(launch_add_count(reinterpret_cast<unsigned long long*>(ix->status + 2), b.fail, st));
+    tm->rec(4, st);
+    return CURPLSH_OK;
+  }
   tm->rec(4, st);
   if (m.checks) *fail_out = b.fail;
   return CURPLSH_OK;
@@ -656,7 +678,7 @@ int search_failed(curplsh_index* ix, int nf, const int* fail_dev, const float* q
   Timing none;
   int* again = nullptr;
   int rc = search_device(ix, nf, qf, k, form, rerank_factor, oif, odf, st, base + qbytes + obytes, &none, false,
-                         false, &again);
+                         false, &again, false);
   if (rc) return rc;
   CUDA_TRY(launch_scatter_results(oif, odf, fail_dev + 2, nf, k, out_idx, out_dist, st));
   return CURPLSH_OK;
@@ -688,17 +710,22 @@ int do_search(curplsh_index* ix, int64_t num, const float* queries, int k, int p
   const bool q_dev = pointer_device(queries) == dev;
   const bool i_dev = pointer_device(indices) == dev;
   const bool d_dev = pointer_device(distances) == dev;
-  // A search that starts from an estimated bound checks it on the host (a
-  // failed query is searched again), so it always returns synchronised.  The
-  // switch is read once here: planning and the check below agree.
-  // Likewise the coarse-margin check of the BF16/FP8 forms: a query it lists
-  // is searched again in the exact form before the call returns.
+  // A search that starts from an estimated bound must check it (a failed
+  // query is searched again).  With the caller's buffers on the device and no
+  // coarse check, the check runs on the stream (search_device) and the call
+  // stays asynchronous; otherwise the host checks it and searches the failed
+  // queries again before returning.  The switches are read once here: planning
+  // and the checks below agree.  The coarse-margin check of the BF16/FP8 forms
+  // is always the host's: a query it lists is searched again in the exact form
+  // before the call returns.
   const bool coarse_on = g_coarse_check.load(std::memory_order_relaxed) != 0;
   const int kp = ix->n > 0 ? kprime_for(form, k, rf, ix->n, coarse_on) : 0;
   const bool est = g_bound_estimate.load(std::memory_order_relaxed) && ix->n > 0 &&
                    plan_estimate(nq, ix->n, kp, ix->dres->num_sms).on;
   const bool coarse = coarse_check_applies(ix, form, kp, coarse_on);
-  const bool sync = force_sync || est || coarse || !(q_dev && i_dev && d_dev);
+  const bool all_dev = q_dev && i_dev && d_dev;
+  const bool dev_recheck = est && !coarse && all_dev && !force_sync;
+  const bool sync = force_sync || (est && !dev_recheck) || coarse || !all_dev;
 
   auto& slot = ix->ws[st];
   if (!slot) slot.reset(new StreamWorkspace());
@@ -736,7 +763,7 @@ int do_search(curplsh_index* ix, int64_t num, const float* queries, int k, int p
   if (!q_dev)
     CUDA_TRY(cudaMemcpyAsync(const_cast<float*>(qd), queries, qbytes, cudaMemcpyDefault, st));
   int* fail = nullptr;
-  int rc = search_device(ix, nq, qd, k, form, rf, oi, od, st, base + off, &tm, est, coarse, &fail);
+  int rc = search_device(ix, nq, qd, k, form, rf, oi, od, st, base + off, &tm, est, coarse, &fail, dev_recheck);
   if (rc) return rc;
   auto copy_out = [&]() -> int {
     if (!(i_dev && d_dev)) {
@@ -971,8 +998,8 @@ int curplsh_index_bf_create(curplsh_resources* r, int dim, const curplsh_bf_conf
   ix->ld8 = round_up(dim, 16);
   r->refs.fetch_add(1);
   DeviceScope scope(c.device);
-  cudaError_t e = cudaMalloc(&ix->status, 2 * sizeof(uint32_t));
-  if (e == cudaSuccess) e = cudaMemset(ix->status, 0, 2 * sizeof(uint32_t));
+  cudaError_t e = cudaMalloc(&ix->status, 4 * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemset(ix->status, 0, 4 * sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ix->order_ev, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ix->fp8_ev, cudaEventDisableTiming);
   if (e != cudaSuccess) {
@@ -1197,7 +1224,13 @@ int curplsh_estimate_plan_shape(int64_t num_rows, int64_t num_queries, int kprim
 
 int curplsh_index_get_fallback_count(curplsh_index* ix, int64_t* count) {
   if (!ix || !count) return set_error(CURPLSH_ERR_INVALID_ARG, "null argument");
-  *count = ix->fallback_queries.load(std::memory_order_relaxed);
+  // searches checked on the host count there; searches checked on their stream
+  // count on the device (read after everything queued so far has run)
+  DeviceScope scope(ix->cfg.device);
+  unsigned long long dev = 0;
+  CUDA_TRY(cudaDeviceSynchronize());
+  CUDA_TRY(cudaMemcpy(&dev, ix->status + 2, sizeof(dev), cudaMemcpyDeviceToHost));
+  *count = ix->fallback_queries.load(std::memory_order_relaxed) + (int64_t)dev;
   return CURPLSH_OK;
 }
 

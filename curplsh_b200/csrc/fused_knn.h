@@ -189,6 +189,7 @@ constexpr int kCheckCoarse = 2;    // coarse (BF16/FP8) distances: verify the ca
 
 struct MergeLaunch {
   int nq, nb, d, k, kprime, pool_cap;
+  const int* run_if = nullptr;   // non-null: the launch does nothing unless *run_if != 0
   int checks = 0;                // kCheck* bits; any bit needs fail_count / fail_list
   int* coarse_count = nullptr;   // kCheckCoarse: queries listed by that check (may be null)
   FusedPlan plan;
@@ -252,6 +253,8 @@ cudaError_t prepare_merge_kernel();
 cudaError_t launch_fill_results(int* idx, float* dist, long long n, cudaStream_t st);
 // p[i] = v for i < n, only when *cond != 0 (decided on the device).
 cudaError_t launch_fill_u32_if(uint32_t* p, long long n, uint32_t v, const int* cond, cudaStream_t st);
+// *acc += *cnt on the stream (one thread)
+cudaError_t launch_add_count(unsigned long long* acc, const int* cnt, cudaStream_t st);
 // out[q] = order bits of the j-th smallest (1-based) of minima[q * count ..
 // q * count + count) for q < nq (all ones when count < j).
 cudaError_t launch_estimate_select(const float* minima, int count, int nq, int j, uint32_t* out, cudaStream_t st);

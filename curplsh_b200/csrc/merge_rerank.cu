@@ -473,7 +473,7 @@ cudaError_t launch_merge_rerank(const MergeLaunch& m, cudaStream_t st) {
   it.ld16 = m.ld16;
   it.out_idx = m.out_idx;
   it.out_dist = m.out_dist;
-  return launch_merge_batch(&it, 1, m.d, m.status, st);
+  return launch_merge_batch(&it, 1, m.d, m.status, st, m.run_if);
 }
 
 }  // namespace curplsh_b200

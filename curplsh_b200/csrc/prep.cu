@@ -240,6 +240,10 @@ __global__ void fill_results_kernel(int* idx, float* dist, long long n) {
   }
 }
 
+__global__ void add_count_kernel(unsigned long long* acc, const int* cnt) {
+  if (*cnt) *acc += (unsigned long long)*cnt;
+}
+
 __global__ void fill_u32_if_kernel(uint32_t* p, long long n, uint32_t v, const int* cond) {
   if (*cond == 0) return;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -381,6 +385,11 @@ cudaError_t launch_fill_u32_if(uint32_t* p, long long n, uint32_t v, const int* 
   long long blocks = (n + 255) / 256;
   if (blocks > 1024) blocks = 1024;
   fill_u32_if_kernel<<<(unsigned)blocks, 256, 0, st>>>(p, n, v, cond);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_add_count(unsigned long long* acc, const int* cnt, cudaStream_t st) {
+  add_count_kernel<<<1, 1, 0, st>>>(acc, cnt);
   return cudaGetLastError();
 }
 

@@ -292,9 +292,11 @@ int curplsh_tuning_clear(void);
  * and start every candidate pool of the full pass at the j-th smallest of those block minima,
  * so far fewer rows survive the filter.  The merge pass verifies the estimate exactly (k'
  * candidates under the final bound prove the result complete); queries it fails are searched
- * again without it before the call returns, so results are identical with the estimate on or
- * off.  A search that uses it returns synchronised even with device buffers.  The switch is
- * process-wide; on (1) by default. */
+ * again without it, so results are identical with the estimate on or off.  With queries,
+ * indices and distances all in device memory and no coarse-margin check (the FP32-exact form,
+ * or the check off) the verification runs on the stream (if any query failed, the full pass and
+ * merge run again from no bound) and the call stays asynchronous; otherwise the host verifies it
+ * and the call returns synchronised.  The switch is process-wide; on (1) by default. */
 int curplsh_set_bound_estimate(int enabled);
 int curplsh_get_bound_estimate(int* enabled);
 /* The estimate a search of num_queries queries with this k / precision / rerank factor would

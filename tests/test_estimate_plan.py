@@ -1,6 +1,6 @@
 """CPU: sizing of the sampled bound estimate (host logic, no device needed).
 
-The plan is restated here from its model: a strided sample holding mu <= 24 of a
+The plan is restated here from its model: a strided sample holding mu <= 12 of a
 query's k' nearest rows on average, at most a tenth of the database's 256-row
 tiles, none below mu = 8 or for N < 2^16 or N < 64 k'; the sample's 128-row
 block minima below the query's k'-th distance are Binomial(B, 1 - (1 - k'/N)^128),
@@ -21,7 +21,7 @@ def model(n, kp):
     if n < (1 << 16) or n < 64 * kp:
         return None
     T = -(-n // 256)
-    tiles = min(math.ceil(24.0 * n / kp / 256), T // 10)
+    tiles = min(math.ceil(12.0 * n / kp / 256), T // 10)
     if kp * tiles * 256 / n < 8.0:
         return None
     rows = tiles * 256

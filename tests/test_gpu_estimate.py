@@ -125,3 +125,41 @@ def test_estimate_switch(cb):
     assert cb.get_bound_estimate() is False
     cb.set_bound_estimate(True)
     assert cb.get_bound_estimate() is True
+
+
+@pytest.mark.parametrize("precision,k", CASES)
+def test_estimate_failure_checked_on_the_stream(cb, res, precision, k):
+    """The same forced failures with queries and results in device memory (and
+    the coarse check off): the check runs on the stream -- the whole pass runs
+    again from no bound -- and the results still equal the search without the
+    estimate; the failed queries are counted on the device."""
+    import torch
+    rng = np.random.default_rng(31 + precision)
+    ix = cb.IndexBF(res, D, cb.IndexBFConfig(precision=precision, rerankFactor=4))
+    ix.add(N, rng.normal(0.0, 1.0, (N, D)).astype(np.float32))
+    rows, step, _ = ix.estimate_plan(NQ, k, precision)
+    assert rows > 0
+    far = np.full(D, 6.0, np.float32)
+    base = (far + rng.normal(0.0, 2.0, (N, D))).astype(np.float32)
+    base[np.arange(rows, dtype=np.int64) * step] = rng.normal(0.0, 0.5, (rows, D)).astype(np.float32)
+    n_near = NQ // 2
+    queries = np.concatenate([rng.normal(0.0, 0.5, (n_near, D)),
+                              far + rng.normal(0.0, 2.0, (NQ - n_near, D))]).astype(np.float32)
+    ix.reset()
+    ix.add(N, base)
+    qd = torch.tensor(queries, device="cuda")
+    oi = torch.empty((NQ, k), dtype=torch.int32, device="cuda")
+    od = torch.empty((NQ, k), dtype=torch.float32, device="cuda")
+    st = torch.cuda.Stream()
+    before = ix.fallback_count()
+    cb.set_bound_estimate(True)
+    ix.search_ex(NQ, qd, k, oi, od, precision, -1, stream=st)
+    st.synchronize()
+    delta = ix.fallback_count() - before
+    cb.set_bound_estimate(False)
+    d0, i0 = ix.search_array(queries, k, precision=precision)
+    cb.set_bound_estimate(True)
+    np.testing.assert_array_equal(oi.cpu().numpy(), i0)
+    np.testing.assert_array_equal(od.cpu().numpy(), d0)
+    assert delta == n_near, (delta, n_near)
+    ix.close()
