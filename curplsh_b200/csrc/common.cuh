@@ -74,6 +74,17 @@ constexpr int kNumThreads = 320;  // warp 0 TMA producer, warp 1 MMA issuer, war
 // and the accumulator is ||q||^2 + ||x||^2 - 2 q.x directly.
 constexpr int kAugCols = 6;
 constexpr int kEpiWarps = 8;
+// Epilogue warps of the candidate-pool kernel, a build option: 8 or 12 (two or
+// three per TMEM lane group; with 12 the block of 14 warps caps registers at
+// 128 a thread).  The block-minimum kernel keeps 8.
+#ifndef CURPLSH_EPI_WARPS
+#define CURPLSH_EPI_WARPS 8
+#endif
+constexpr int kPoolEpiWarps = CURPLSH_EPI_WARPS;
+static_assert(kPoolEpiWarps == 8 || kPoolEpiWarps == 12, "8 or 12 epilogue warps");
+constexpr int kMaxEpiWarps = 12;
+__host__ __device__ constexpr int epi_warps_for(bool minima) { return minima ? kEpiWarps : kPoolEpiWarps; }
+__host__ __device__ constexpr int threads_for(bool minima) { return 64 + 32 * epi_warps_for(minima); }
 constexpr int kPoolRoom = kBN;  // free slots a candidate pool keeps for the next tile (both halves)
 // Tiles between two selection points of a shared candidate pool: two when the
 // capacity leaves room for two tiles of appends above k' + 128, else one.

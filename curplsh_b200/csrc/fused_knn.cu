@@ -98,8 +98,9 @@ struct SmemLayout {
   uint32_t b_tail;     // bytes of the B tail chunk
 };
 
-// pair = 1: this CTA holds half of each 256-row database tile (CTA pairs).
-__host__ __device__ inline SmemLayout make_layout(int form, int d, int pair = 0) {
+// pair = 1: this CTA holds half of each 256-row database tile (CTA pairs);
+// epi_warps: epilogue warps (each has a 1 KB histogram / staging area).
+__host__ __device__ inline SmemLayout make_layout(int form, int d, int pair = 0, int epi_warps = kEpiWarps) {
   SmemLayout L{};
   L.b_chunk = pair ? kBChunkBytes / 2 : kBChunkBytes;
   L.b_tail = pair ? kBTailBytes / 2 : kBTailBytes;
@@ -113,7 +114,7 @@ __host__ __device__ inline SmemLayout make_layout(int form, int d, int pair = 0)
   // the tail runs the hi x hi product alone, which is exact only for those
   L.tail_narrow = folded && (d % 64 == 0);
   // everything below the barrier block must fit the 227 KB opt-in limit
-  const uint32_t budget = 227u * 1024u - 256u - (uint32_t)kEpiWarps * 256u * 4u - 1024u - 1024u;
+  const uint32_t budget = 227u * 1024u - 256u - (uint32_t)epi_warps * 256u * 4u - 1024u - 1024u;
   const int nreg = L.nkc - (L.tail_narrow ? 1 : 0);
   const uint32_t a_res = (uint32_t)nreg * a_parts * kAChunkBytes + (L.tail_narrow ? kATailBytes : 0u);
   // a stage = one regular K chunk of the tile; the last one also carries the tail
@@ -132,7 +133,7 @@ __host__ __device__ inline SmemLayout make_layout(int form, int d, int pair = 0)
   L.stages = s < 2 ? 2 : (s > 8 ? 8 : s);
   L.bar_off = L.a_bytes + (uint32_t)L.stages * L.stage_bytes;
   L.hist_off = L.bar_off + 256;  // barriers: 2*8 + 6 mbarriers + tmem slot + flags < 256 B
-  L.pool_off = L.hist_off + kEpiWarps * 256 * 4;
+  L.pool_off = L.hist_off + epi_warps * 256 * 4;
   L.total = L.pool_off + 1024 + 1024;
   return L;
 }
@@ -361,7 +362,7 @@ __device__ __forceinline__ float select32(const float (&v)[32], int j) {
 // instructions can only be launched as clusters of two, so the single-CTA
 // kernel is a separate instance without them.
 template <int FORM, int MAXI, bool MINIMA = false, bool PAIR = false>
-__global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_constant__ FusedArgs<MAXI> A) {
+__global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const __grid_constant__ FusedArgs<MAXI> A) {
   using Tr = FormTraits<FORM>;
   const FusedBatch& B = A.B;
   // a conditional pass (a re-search after a failed check): every thread of
@@ -370,7 +371,9 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
   if (B.run_if && *B.run_if == 0) return;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const SmemLayout L = make_layout(FORM, B.d, PAIR ? 1 : 0);
+  constexpr int EW = epi_warps_for(MINIMA);  // epilogue warps
+  constexpr int WG = EW / 4;                  // epilogue warps per TMEM lane group
+  const SmemLayout L = make_layout(FORM, B.d, PAIR ? 1 : 0, EW);
   const int S = L.stages;
   // CTA pairs: rank 0 issues the MMAs and owns the barriers the pair's loads
   // complete on; each CTA loads and filters its own query block
@@ -404,7 +407,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
     mbar_init(a_empty, 1);
     for (int s = 0; s < 2; ++s) {
       mbar_init(&acc_full[s], 1);
-      mbar_init(&acc_empty[s], pair ? 2 * kEpiWarps : kEpiWarps);  // both CTAs' epilogue warps
+      mbar_init(&acc_empty[s], pair ? 2 * EW : EW);  // both CTAs' epilogue warps
     }
     mbar_init(drain, 1);
     *abort_flag = 0;
@@ -620,18 +623,21 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
     }
   } else {
     // ------------------------------------------------------------ epilogue
-    // Warps ew and ew + 4 read the same TMEM lanes (queries) and split each
-    // tile's columns into halves g = 0, 1.  They share ONE candidate pool per
+    // The WG warps ew, ew + 4, ... read the same TMEM lanes (queries) and split
+    // each tile's four 64-column chunks between them: with two warps, warp g
+    // takes the 128-column half g; with three, chunk c of the tile counted tc
+    // goes to warp (4 tc + c) mod 3.  They share ONE candidate pool per
     // (query, unit): appends reserve slots with a shared-memory counter, and at
-    // every tile end the pair meets at a named barrier, splits the pools that
-    // need a selection between them, and meets again.  A shared pool sees
-    // both halves' rows, so its bound tightens as one pool over the whole
+    // every S-th tile end the group meets at a named barrier, splits the pools
+    // that need a selection between them, and meets again.  A shared pool sees
+    // all of a tile's rows, so its bound tightens as one pool over the whole
     // tile would -- about half the survivors and selections of a pool per half.
-    const int ew = warp - 2;       // 0..7
-    const int g = ew >> 2;         // which 128-column half of each tile
+    const int ew = warp - 2;       // 0..EW-1
+    const int g = ew >> 2;         // this warp's index within its lane group
     const int lg = warp & 3;       // TMEM lane group this warp may access
     const int row = lg * 32 + lane;
-    const int pair_bar = 1 + lg;   // named barrier of the two warps of lane group lg
+    const int pair_bar = 1 + lg;   // named barrier of the WG warps of lane group lg
+    constexpr int kGroupThreads = 32 * WG;
     uint32_t* hist = hist_all + ew * 256;
     int* cnt_s = reinterpret_cast<int*>(smem + L.pool_off);             // [128] pool counts
     float* thr_s = reinterpret_cast<float*>(smem + L.pool_off) + kBM;   // [128] pool bounds
@@ -678,12 +684,12 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
         cnt_s[row] = 0;
         thr_s[row] = 3.402823466e38f;
       }
-      bar_sync_named(pair_bar, 64);
+      bar_sync_named(pair_bar, kGroupThreads);
       float thr = 3.402823466e38f;  // FLT_MAX: admits every finite distance until a pool fills
 
       // Selections of the pools in `need` (lane bits of this lane group; warp g
-      // owns the pools of lanes with parity g, so the pair never touches the
-      // same pool's state).  Each keeps `keep` keys, records the pool's new
+      // owns the pools of lanes l with l mod WG = g, so two warps never touch
+      // the same pool's state).  Each keeps `keep` keys, records the pool's new
       // count and bound in shared memory and publishes a full set's k'-th
       // distance to q_bound.
       auto refresh = [&](uint32_t need, int keep) {
@@ -717,15 +723,27 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
         if (nb_ob != kOrdInf) thr = fminf(thr, thr_from<Tr::kFolded>(ord2f(nb_ob), qn));
         const float thr_up = next_above(thr);  // d <= thr  <=>  d < thr_up
         if (valid) nb_ob = ld_relaxed_u32(&p.q_bound[q]);
-        // FP8: this half tile's database norms and scales, loaded before the
-        // accumulator wait (their latency overlaps it) and staged in the
+        // this warp's 64-column chunks of the tile (-1: none): 2g and 2g + 1
+        // with two warps per lane group; with three, the c with 4 tc + c = g
+        // (mod 3), i.e. c1 = (g - tc) mod 3 and, when c1 = 0, also 3
+        int my_c[2];
+        if constexpr (WG == 2) {
+          my_c[0] = 2 * g;
+          my_c[1] = 2 * g + 1;
+        } else {
+          my_c[0] = (int)(((uint32_t)g + 3u - tc % 3u) % 3u);
+          my_c[1] = my_c[0] == 0 ? 3 : -1;
+        }
+        // FP8: the database norms and scales of these columns, loaded before
+        // the accumulator wait (their latency overlaps it) and staged in the
         // warp's histogram area, which is free outside a refresh
         float pxn[4], psx[4];
         if (Tr::kFP8) {
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
+            const int cc = my_c[i >> 1] < 0 ? my_c[0] : my_c[i >> 1];
             // < nb_pad: rows are padded to whole tiles (a strided sample has no padding)
-            const int c0 = tphys * kBN + g * kHalfN + lane + 32 * i;
+            const int c0 = tphys * kBN + cc * 64 + lane + 32 * (i & 1);
             const size_t c = MINIMA ? (size_t)c0 * (size_t)p.db_step : (size_t)c0;
             pxn[i] = __ldg(p.db_norms + c);
             psx[i] = __ldg(p.db_scale + c);
@@ -739,7 +757,6 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
         if (got) {
         STAT_BEGIN(tfl);
         tc_fence_after();
-        const int colh = tphys * kBN + g * kHalfN;
         float bmin = 3.402823466e38f;  // block-minimum mode: smallest distance of this half tile
         float* colv = reinterpret_cast<float*>(hist);  // [128] norms, then [128] scales
         if (Tr::kFP8) {
@@ -752,13 +769,15 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
           __syncwarp();
         }
 #pragma unroll 1
-        for (int h = 0; h < kHalfN / 64; ++h) {
+        for (int h = 0; h < 2; ++h) {
+          const int ch = my_c[h];
+          if (ch < 0) break;
           uint32_t v[64];
           STAT_BEGIN(ttm);
-          tmem_ld_32x32b_x64(tmem_base + lane_base + slot * kBN + g * kHalfN + h * 64, v);
+          tmem_ld_32x32b_x64(tmem_base + lane_base + slot * kBN + ch * 64, v);
           tmem_ld_wait();
           STAT_END(ttm, st_tmem);
-          const int col0 = colh + h * 64;
+          const int col0 = tphys * kBN + ch * 64;
           // coarse distances of the 64 columns (two independent 32-column halves)
           float da[32], db[32];
           if (Tr::kFolded) {
@@ -910,7 +929,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
         // together if either aborted
         if ((t - t0 + 1) % S != 0 && t + 1 < t1) continue;
         STAT_BEGIN(tb1);
-        const bool leave = bar_red_or(pair_bar, 64, !got || *abort_flag != 0);
+        const bool leave = bar_red_or(pair_bar, kGroupThreads, !got || *abort_flag != 0);
         STAT_END(tb1, st_bar);
         if (leave) {
           ok = false;
@@ -920,12 +939,12 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
         // or, at the unit's end, every pool above k' (the merge pass reads at
         // most k' keys' worth beyond what it needs)
         const int lim = t + 1 < t1 ? P - S * kBN : p.kprime;
-        const bool mine = (lane & 1) == g;
+        const bool mine = (lane % WG) == g;
         const int cn = mine ? cnt_s[row] : 0;
         if (cn > P) atomicOr(B.status, kErrPoolOverflow);
         refresh(__ballot_sync(0xffffffffu, mine && valid && cn > lim), p.kprime);
         STAT_BEGIN(tb2);
-        bar_sync_named(pair_bar, 64);
+        bar_sync_named(pair_bar, kGroupThreads);
         STAT_END(tb2, st_bar);
       }
       if (!ok) break;
@@ -936,7 +955,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) fused_knn_kernel(const __grid_
         p.pool_counts[(pool_row0 + row) * U + u_ord] = cn < P ? cn : P;
         if (gap) p.pool_counts[(pool_row0 + row) * U + u_ord - 1] = 0;
       }
-      bar_sync_named(pair_bar, 64);  // the counts are read before the next unit resets them
+      bar_sync_named(pair_bar, kGroupThreads);  // the counts are read before the next unit resets them
     }
     if (lane == 0) {
       STAT_FLUSH(kStatEpiWaitAccFull, st_wait);
@@ -1029,6 +1048,7 @@ cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, 
                         const int* run_if) {
   cudaError_t e = ensure_attributes<FORM, MAXI, MINIMA, PAIR>();
   if (e != cudaSuccess) return e;
+  smem = make_layout(FORM, specs[0].d, PAIR ? 1 : 0, epi_warps_for(MINIMA)).total;  // this instance's layout
   FusedArgs<MAXI> a;
   memset(&a, 0, sizeof(a));
   a.B.num_items = n;
@@ -1091,13 +1111,13 @@ cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, 
     }
   }
   if (!PAIR) {
-    fused_knn_kernel<FORM, MAXI, MINIMA, PAIR><<<bp.grid, kNumThreads, smem, st>>>(a);
+    fused_knn_kernel<FORM, MAXI, MINIMA, PAIR><<<bp.grid, threads_for(MINIMA), smem, st>>>(a);
     return cudaGetLastError();
   }
   if (bp.grid % 2) return cudaErrorInvalidValue;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)bp.grid, 1, 1);
-  cfg.blockDim = dim3(kNumThreads, 1, 1);
+  cfg.blockDim = dim3(threads_for(MINIMA), 1, 1);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
