@@ -226,8 +226,10 @@ struct curplsh_index {
   __nv_bfloat16* xl = nullptr;    // [n_pad x ld16]
   uint8_t* x8 = nullptr;          // [n_pad x ld8]   (built on first FP8 search)
   float* xs = nullptr;            // [n_pad]
+  float xs_uniform = 0.f;         // > 0: every row of the FP8 copy has this scale
   uint32_t* status = nullptr;     // device words: [0] error status, [1] nonzero if a row is not exactly BF16,
-                                  // [2..3] 64-bit count of queries whose estimate failed in device-checked searches
+                                  // [2..3] 64-bit count of queries whose estimate failed in device-checked searches,
+                                  // [4..5] range of the FP8 row scales while the copy is built
   bool bf16_exact = false;        // every stored value is exactly a BF16 value (rerank reads xh)
   long long generation = 0;       // bumped whenever the prepared database changes (add, reset)
   cudaEvent_t order_ev = nullptr; // orders default-stream searches after the legacy stream
@@ -246,6 +248,7 @@ struct curplsh_index {
     xh = xl = nullptr;
     x8 = nullptr;
     xs = nullptr;
+    xs_uniform = 0.f;
     n = 0;
     n_pad = 0;
   }
@@ -257,6 +260,16 @@ namespace {
 // wait for it.  The copy is written asynchronously, so a reader on any other
 // stream must wait on fp8_ev (recorded right after the write) before it reads
 // x8/xs; searches on `st` itself are ordered by the stream.
+//
+// Row scales: each row's own (max |x| / 448) unless the nonzero rows' scales
+// all lie within a factor kFP8UniformSpan of each other; then every row takes
+// the largest.  E4M3 is a floating-point format, so a row whose own scale is
+// at most 16x smaller keeps its elements in the normal range (2^-6 .. 448)
+// either way, and a common scale lets the FP8 pass compare
+// ||x||^2 - 2 s_q s acc without loading a scale per database row.  Deciding
+// reads two words on the host once per build.
+constexpr float kFP8UniformSpan = 16.f;
+
 int build_fp8(curplsh_index* ix, cudaStream_t st) {
   if (ix->n == 0) return CURPLSH_OK;
   if (!ix->x8) {
@@ -264,6 +277,21 @@ int build_fp8(curplsh_index* ix, cudaStream_t st) {
     CUDA_TRY(cudaMalloc(&ix->xs, (size_t)ix->n_pad * sizeof(float)));
     CUDA_TRY(launch_prep_rows(ix->x32, ix->dim, (int)ix->n, ix->n_pad, ix->dim, nullptr, 0.f, nullptr, nullptr,
                               ix->ld16, ix->x8, ix->xs, ix->ld8, st));
+    uint32_t range[2] = {0xFFFFFFFFu, 0u};
+    CUDA_TRY(launch_positive_range(ix->xs, ix->n, ix->status + 4, st));
+    CUDA_TRY(cudaMemcpyAsync(range, ix->status + 4, sizeof(range), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    ix->xs_uniform = 0.f;
+    if (range[1] > 0u && range[0] <= range[1]) {
+      float lo, hi;
+      memcpy(&lo, &range[0], sizeof(float));
+      memcpy(&hi, &range[1], sizeof(float));
+      if (hi <= kFP8UniformSpan * lo) {
+        CUDA_TRY(launch_prep_rows(ix->x32, ix->dim, (int)ix->n, ix->n_pad, ix->dim, nullptr, 0.f, nullptr, nullptr,
+                                  ix->ld16, ix->x8, ix->xs, ix->ld8, st, kAugNone, nullptr, hi));
+        ix->xs_uniform = hi;
+      }
+    }
     CUDA_TRY(cudaEventRecord(ix->fp8_ev, st));
     return CURPLSH_OK;
   }
@@ -560,6 +588,7 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
   f.x8 = ix->x8;
   f.xn = ix->xn;
   f.xs = ix->xs;
+  f.xs_uniform = ix->xs_uniform;
   f.pools = b.pools;
   f.pool_counts = b.counts;
   f.q_bound = b.qbound;
@@ -839,6 +868,7 @@ int index_lock_view(curplsh_index* ix, IndexView* v) {
   v->xl = ix->xl;
   v->x8 = ix->x8;
   v->xs = ix->xs;
+  v->xs_uniform = ix->xs_uniform;
   v->generation = ix->generation;
   v->bf16_exact = ix->bf16_exact;
   v->stream = ix->dres->def;
@@ -854,6 +884,7 @@ int index_prepare_form(curplsh_index* ix, int form, IndexView* v) {
   CUDA_TRY(cudaStreamSynchronize(ix->dres->def));
   v->x8 = ix->x8;
   v->xs = ix->xs;
+  v->xs_uniform = ix->xs_uniform;
   return CURPLSH_OK;
 }
 int search_kprime(int form, int k, int rerank_factor, long long n) {
@@ -998,8 +1029,8 @@ int curplsh_index_bf_create(curplsh_resources* r, int dim, const curplsh_bf_conf
   ix->ld8 = round_up(dim, 16);
   r->refs.fetch_add(1);
   DeviceScope scope(c.device);
-  cudaError_t e = cudaMalloc(&ix->status, 4 * sizeof(uint32_t));
-  if (e == cudaSuccess) e = cudaMemset(ix->status, 0, 4 * sizeof(uint32_t));
+  cudaError_t e = cudaMalloc(&ix->status, 6 * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemset(ix->status, 0, 6 * sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ix->order_ev, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ix->fp8_ev, cudaEventDisableTiming);
   if (e != cudaSuccess) {

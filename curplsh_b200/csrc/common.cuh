@@ -113,7 +113,7 @@ struct FusedItem {
   int* pool_counts;        // [G_i*128][U_i]
   uint32_t* q_bound;       // [nq_pad] shared per-query bound (ordered bits), init kOrdInf or an estimate
   int db_step;             // database row j of this item is stored row j * db_step (>= 1)
-  int reserved;
+  float db_scale_uniform;  // > 0: every database row has this FP8 scale (db_scale is not read)
   // Non-null: block-minimum mode (no pools): minima[q * 2 * num_tiles + 2 * t + h]
   // gets the smallest key distance of query q over rows [256 t + 128 h, +128).
   float* minima;

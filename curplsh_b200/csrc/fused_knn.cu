@@ -673,6 +673,9 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
       const float qn = valid ? p.q_norms[q] : 0.f;
       float m2s = -2.f;
       if (Tr::kFP8) m2s = valid ? -2.f * p.q_scale[q] : 0.f;
+      // FP8 with one scale s for every database row: d = ||x||^2 + (-2 s_q s) acc
+      const bool uniform = Tr::kFP8 && p.db_scale_uniform > 0.f;
+      const float ku = m2s * p.db_scale_uniform;
       const size_t pool_row0 = (size_t)qb * kBM;  // pool index of lane-group row 0 is added per lane
       auto pool_of = [&](int r) -> uint64_t* {
         return p.pools + ((pool_row0 + (size_t)r) * U + (size_t)u_ord) * (size_t)P;
@@ -746,7 +749,7 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
             const int c0 = tphys * kBN + cc * 64 + lane + 32 * (i & 1);
             const size_t c = MINIMA ? (size_t)c0 * (size_t)p.db_step : (size_t)c0;
             pxn[i] = __ldg(p.db_norms + c);
-            psx[i] = __ldg(p.db_scale + c);
+            psx[i] = uniform ? 0.f : __ldg(p.db_scale + c);
           }
         }
         STAT_BEGIN(tw);
@@ -790,6 +793,18 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
           } else {
             const float4* xn4 = reinterpret_cast<const float4*>(colv + h * 64);
             const float4* sx4 = reinterpret_cast<const float4*>(colv + kHalfN + h * 64);
+            if (uniform) {
+#pragma unroll
+              for (int j4 = 0; j4 < 16; ++j4) {
+                const float4 xn = xn4[j4];
+                float* dst = j4 < 8 ? da : db;
+                const int o = (j4 & 7) * 4;
+                fma2_f32(dst[o + 0], dst[o + 1], __uint_as_float(v[4 * j4 + 0]), __uint_as_float(v[4 * j4 + 1]), ku,
+                         ku, xn.x, xn.y);
+                fma2_f32(dst[o + 2], dst[o + 3], __uint_as_float(v[4 * j4 + 2]), __uint_as_float(v[4 * j4 + 3]), ku,
+                         ku, xn.z, xn.w);
+              }
+            } else
 #pragma unroll
             for (int j4 = 0; j4 < 16; ++j4) {
               const float4 xn = xn4[j4];
@@ -1084,6 +1099,7 @@ cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, 
     it.pool_counts = f.pool_counts;
     it.q_bound = f.q_bound;
     it.db_step = f.db_step > 1 ? f.db_step : 1;
+    it.db_scale_uniform = f.xs_uniform;
     it.minima = f.minima;
     CUtensorMap* m = &a.maps[i * kMapsPerItem];
     const void* qh = fp8 ? (const void*)f.q8 : (const void*)f.qh;
@@ -1292,6 +1308,7 @@ cudaError_t launch_fused(const FusedLaunch& f, cudaStream_t st) {
   s.x8 = f.x8;
   s.xn = f.xn;
   s.xs = f.xs;
+  s.xs_uniform = f.xs_uniform;
   s.pools = f.pools;
   s.pool_counts = f.pool_counts;
   s.q_bound = f.q_bound;

@@ -56,6 +56,7 @@ struct FusedLaunch {
   const uint8_t* x8;
   const float* xn;
   const float* xs;
+  float xs_uniform = 0.f;   // > 0: one FP8 scale for every database row
   // database row j of this pass is stored row j * db_step (a strided sample when > 1)
   int db_step = 1;
   // non-null: block-minimum mode, see FusedItem::minima (pools are not used)
@@ -97,6 +98,7 @@ struct FusedItemSpec {
   const uint8_t* x8;
   const float* xn;
   const float* xs;
+  float xs_uniform;         // > 0: one FP8 scale for every database row
   uint64_t* pools;          // [G*128][U][pool_cap]
   int* pool_counts;         // [G*128][U]
   uint32_t* q_bound;        // [nq_pad], initialised to all ones (or to estimated bounds)
@@ -160,7 +162,10 @@ enum AugMode : int { kAugNone = 0, kAugDatabase = 1, kAugQuery = 2 };
 cudaError_t launch_prep_rows(const float* x, long long ldx, int nrows, long long nrows_pad, int d, float* norms,
                              float pad_norm, __nv_bfloat16* hi, __nv_bfloat16* lo, long long ld16, uint8_t* f8,
                              float* scale, long long ld8, cudaStream_t st, int aug = kAugNone,
-                             uint32_t* lo_nonzero = nullptr);
+                             uint32_t* lo_nonzero = nullptr, float fixed_scale = 0.f);
+// out[0] / out[1] = order bits of the smallest / largest positive s[i], i < n
+// (0xFFFFFFFF / 0 when there is none)
+cudaError_t launch_positive_range(const float* s, long long n, uint32_t* out, cudaStream_t st);
 
 // The same preparation for several row ranges of one dimension in a single
 // launch.  Every pointer points at the segment's first row; source rows have
@@ -280,6 +285,7 @@ struct IndexView {
   const __nv_bfloat16* xl;
   const uint8_t* x8;
   const float* xs;
+  float xs_uniform;      // > 0: every row of the FP8 copy has this scale
   long long generation;  // changes whenever add()/reset() replace the prepared database
   bool bf16_exact;       // every stored value is exactly a BF16 value (xl is all zero)
   cudaStream_t stream;   // the index's default stream

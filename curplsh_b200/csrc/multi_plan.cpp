@@ -226,6 +226,7 @@ void MultiPlan::bind(void* base_v) {
     s.x8 = v.x8;
     s.xn = v.xn;
     s.xs = v.xs;
+    s.xs_uniform = v.xs_uniform;
     s.pool_counts = reinterpret_cast<int*>(base + x.o_counts);
     s.pools = reinterpret_cast<uint64_t*>(base + x.o_pools);
   }
@@ -314,6 +315,7 @@ int MultiPlan::enqueue(cudaStream_t main, const std::vector<cudaStream_t>* branc
       e.x8 = s.x8;
       e.xn = s.xn;
       e.xs = s.xs;
+      e.xs_uniform = s.xs_uniform;
       e.db_step = x.est.step;
       e.minima = reinterpret_cast<float*>(base_ + x.o_minima);
       e.pools = s.pools;

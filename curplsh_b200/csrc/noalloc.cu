@@ -213,6 +213,7 @@ int search_noalloc_locked(const IndexView& v, int nq, const float* q, int k, int
   f.x8 = v.x8;
   f.xn = v.xn;
   f.xs = v.xs;
+  f.xs_uniform = v.xs_uniform;
   f.pools = pools;
   f.pool_counts = counts;
   f.q_bound = qbound;

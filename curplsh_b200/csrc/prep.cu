@@ -56,7 +56,7 @@ __device__ __forceinline__ void prep_row(const float* __restrict__ x, long long 
                                          float* __restrict__ norms, float pad_norm, __nv_bfloat16* __restrict__ hi,
                                          __nv_bfloat16* __restrict__ lo, long long ld16, uint8_t* __restrict__ f8,
                                          float* __restrict__ scale, long long ld8, int vec4, int aug,
-                                         uint32_t* __restrict__ lo_nonzero = nullptr) {
+                                         uint32_t* __restrict__ lo_nonzero = nullptr, float fixed_scale = 0.f) {
   const int lane = threadIdx.x & 31;
   if (r >= nrows) {
     if (norms && lane == 0) norms[r] = pad_norm;
@@ -97,9 +97,10 @@ __device__ __forceinline__ void prep_row(const float* __restrict__ x, long long 
   float inv = 1.f;
   if (f8) {
     m = warp_max(m);
-    const float sc = m > 0.f ? m / kE4M3Max : 1.f;
-    inv = 1.f / sc;
-    if (scale && lane == 0) scale[r] = sc;
+    // an all-zero row gets scale 0 (its codes are 0 whatever the scale)
+    const float sc = fixed_scale > 0.f ? fixed_scale : m / kE4M3Max;
+    inv = sc > 0.f ? 1.f / sc : 0.f;
+    if (scale && lane == 0) scale[r] = m > 0.f ? sc : 0.f;
   }
   if (vec4) {
     const float4* row4 = reinterpret_cast<const float4*>(row);
@@ -174,10 +175,33 @@ __global__ void __launch_bounds__(kPrepWarps * 32) prep_rows_kernel(
     const float* __restrict__ x, long long ldx, int nrows, long long nrows_pad, int d, float* __restrict__ norms,
     float pad_norm, __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, long long ld16,
     uint8_t* __restrict__ f8, float* __restrict__ scale, long long ld8, int vec4, int aug,
-    uint32_t* __restrict__ lo_nonzero) {
+    uint32_t* __restrict__ lo_nonzero, float fixed_scale) {
   const long long r = (long long)blockIdx.x * kPrepWarps + (threadIdx.x >> 5);
   if (r >= nrows_pad) return;
-  prep_row(x, ldx, r, nrows, d, norms, pad_norm, hi, lo, ld16, f8, scale, ld8, vec4, aug, lo_nonzero);
+  prep_row(x, ldx, r, nrows, d, norms, pad_norm, hi, lo, ld16, f8, scale, ld8, vec4, aug, lo_nonzero, fixed_scale);
+}
+
+// Smallest and largest positive value of s[0, n) as order bits (positive
+// floats order as unsigned integers): out[0] = min (start 0xFFFFFFFF),
+// out[1] = max (start 0).
+__global__ void positive_range_kernel(const float* __restrict__ s, long long n, uint32_t* __restrict__ out) {
+  uint32_t lo = 0xFFFFFFFFu, hi = 0u;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float v = s[i];
+    if (v > 0.f) {
+      lo = min(lo, __float_as_uint(v));
+      hi = max(hi, __float_as_uint(v));
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&out[0], lo);
+    atomicMax(&out[1], hi);
+  }
 }
 
 struct PrepSegmentArgs {
@@ -339,12 +363,24 @@ __global__ void scatter_results_kernel(const int* __restrict__ in_idx, const flo
 
 cudaError_t launch_prep_rows(const float* x, long long ldx, int nrows, long long nrows_pad, int d, float* norms,
                              float pad_norm, __nv_bfloat16* hi, __nv_bfloat16* lo, long long ld16, uint8_t* f8,
-                             float* scale, long long ld8, cudaStream_t st, int aug, uint32_t* lo_nonzero) {
+                             float* scale, long long ld8, cudaStream_t st, int aug, uint32_t* lo_nonzero,
+                             float fixed_scale) {
   if (nrows_pad <= 0) return cudaSuccess;
   const int vec4 = (d % 4 == 0) && (ldx % 4 == 0) && ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
   const long long blocks = (nrows_pad + kPrepWarps - 1) / kPrepWarps;
   prep_rows_kernel<<<(unsigned)blocks, kPrepWarps * 32, 0, st>>>(x, ldx, nrows, nrows_pad, d, norms, pad_norm, hi,
-                                                                 lo, ld16, f8, scale, ld8, vec4, aug, lo_nonzero);
+                                                                 lo, ld16, f8, scale, ld8, vec4, aug, lo_nonzero,
+                                                                 fixed_scale);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_positive_range(const float* s, long long n, uint32_t* out, cudaStream_t st) {
+  const uint32_t init[2] = {0xFFFFFFFFu, 0u};
+  cudaError_t e = cudaMemcpyAsync(out, init, sizeof(init), cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess || n <= 0) return e;
+  long long blocks = (n + 255) / 256;
+  if (blocks > 1024) blocks = 1024;
+  positive_range_kernel<<<(unsigned)blocks, 256, 0, st>>>(s, n, out);
   return cudaGetLastError();
 }
 
