@@ -116,8 +116,10 @@ def load_traffic(workload, form_name):
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
 
-    def __init__(self, index=0):
+    def __init__(self, index=0, interval_ms=50, settle_s=0.25):
         self.index = index
+        self.interval_ms = interval_ms
+        self.settle_s = settle_s  # nvidia-smi's start-up (device queries) ends before the timed work
         self.proc = None
         self.lines = []
 
@@ -126,14 +128,14 @@ class ClockSampler:
                "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-               "--format=csv,noheader,nounits", "-lms", "50"]
+               "--format=csv,noheader,nounits", "-lms", str(self.interval_ms)]
         try:
             self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except OSError:
             self.proc = None
-        time.sleep(0.25)
+        time.sleep(self.settle_s)
         return self
 
     def _read(self):
@@ -632,7 +634,9 @@ def run_serving(cb, synth, args, world, rank, local, res):
             sizes = request_sizes(count)
             gaps = rng.exponential(1.0 / mean_req, size=count)
             arrivals = np.cumsum(gaps) - gaps[0]
-            sampler = ClockSampler(local)
+            # a slower sampler with a longer settle: each nvidia-smi query takes
+            # driver locks that a latency measurement would otherwise see
+            sampler = ClockSampler(local, interval_ms=200, settle_s=1.0)
             sampler.__enter__()
             lat, wall, (_, _, ph) = run_load(srv, sizes, list(arrivals))
             sampler.__exit__(None, None, None)

@@ -26,7 +26,16 @@ namespace curplsh_b200 {
 
 namespace {
 
-constexpr int kMergeThreads = 256;
+// Threads per query's CTA (a build option: 256 or 128); the radix histogram has
+// 256 bins, 256 / kMergeThreads per thread.  128 threads put twice as many
+// queries in flight per SM at the same register budget (merge of a 10^4-query
+// BF16 search 0.32 -> 0.28 ms).
+#ifndef CURPLSH_MERGE_THREADS
+#define CURPLSH_MERGE_THREADS 128
+#endif
+constexpr int kMergeThreads = CURPLSH_MERGE_THREADS;
+static_assert(kMergeThreads == 256 || kMergeThreads == 128, "256 or 128 merge threads");
+constexpr int kBinsPerThread = 256 / kMergeThreads;
 // Candidates one warp reranks at once: each lane keeps this many database rows
 // in flight (a row of d = 128 is one 16-byte load per lane).
 #ifndef CURPLSH_RERANK_ROWS
@@ -71,19 +80,29 @@ __device__ uint64_t block_select_bound(Each each, uint32_t keep, uint32_t* hist,
   uint64_t prefix = 0, pmask = 0;
   uint32_t rank = keep;
   for (int shift = 56; shift >= 0; shift -= 8) {
-    hist[tid] = 0u;  // kMergeThreads == 256 bins
+#pragma unroll
+    for (int b = 0; b < kBinsPerThread; ++b) hist[tid * kBinsPerThread + b] = 0u;
     __syncthreads();
     each([&](uint64_t key) {
       if ((key & pmask) == prefix) atomicAdd(&hist[(uint32_t)(key >> shift) & 255u], 1u);
     });
     __syncthreads();
-    const uint32_t c = hist[tid];
+    uint32_t cb[kBinsPerThread], c = 0;
+#pragma unroll
+    for (int b = 0; b < kBinsPerThread; ++b) {
+      cb[b] = hist[tid * kBinsPerThread + b];
+      c += cb[b];
+    }
     const uint32_t incl = block_incl_scan(c, warp_tot);
-    const uint32_t excl = incl - c;
-    if (excl < rank && rank <= incl) {
-      misc[1] = (uint32_t)tid;
-      misc[2] = excl;
-      misc[3] = c;
+    uint32_t excl = incl - c;
+#pragma unroll
+    for (int b = 0; b < kBinsPerThread; ++b) {
+      if (excl < rank && rank <= excl + cb[b]) {
+        misc[1] = (uint32_t)(tid * kBinsPerThread + b);
+        misc[2] = excl;
+        misc[3] = cb[b];
+      }
+      excl += cb[b];
     }
     __syncthreads();
     const uint32_t digit = misc[1], before = misc[2], cnt = misc[3];
@@ -98,11 +117,12 @@ __device__ uint64_t block_select_bound(Each each, uint32_t keep, uint32_t* hist,
 
 // Resident CTAs per SM the register allocation must allow: each query's CTA
 // spends most of its time waiting on gathers and barriers, so occupancy hides
-// latency.  Unbounded, the kernel took 96 registers (2 CTAs per SM); at 6 it
-// takes 40 with a few spills and the merge of a 10^4-query search drops from
-// 0.62 to 0.32 ms (BF16, k' = 224).
+// latency.  Unbounded, the 256-thread kernel took 96 registers (2 CTAs per
+// SM); at 6 CTAs (40 registers, a few spills) the merge of a 10^4-query search
+// dropped from 0.62 to 0.32 ms (BF16, k' = 224).  12 for 128 threads: the same
+// 40-register budget.
 #ifndef CURPLSH_MERGE_MIN_BLOCKS
-#define CURPLSH_MERGE_MIN_BLOCKS 6
+#define CURPLSH_MERGE_MIN_BLOCKS (kMergeThreads == 128 ? 12 : 6)
 #endif
 __global__ void __launch_bounds__(kMergeThreads, CURPLSH_MERGE_MIN_BLOCKS)
     merge_rerank_kernel(const __grid_constant__ MergeArgs a) {
