@@ -262,8 +262,10 @@ def run_single(cb, synth, wl, args, world, rank, local, res, peaks, fp8_peak, wi
     dev = f"cuda:{local}"
     info = WORKLOADS[wl]
     n_db, _, dim, _ = synth.CONFIGS[wl]
+    if args.rows:  # a smaller case of the same workload (profiling captures)
+        n_db = args.rows
     # every rank holds the same database and searches a full query batch (replicas)
-    base, queries, k = synth.make(wl, backend="torch", device=dev)
+    base, queries, k = synth.make(wl, backend="torch", device=dev, n=args.rows or None, q=args.queries or None)
     torch.cuda.synchronize()  # generated on torch's stream; the library orders its work on its own streams
     stream = torch.cuda.Stream(device=dev)
     Q = queries.shape[0]
@@ -719,6 +721,9 @@ def main():
     ap.add_argument("--workload", default=WORKLOAD, choices=list(WORKLOADS) + ["batched_uneven", "serving"])
     ap.add_argument("--configs", default=",".join(SUB_CONFIGS),
                     help="per-workload records added to the headline line on one GPU ('none' for none)")
+    ap.add_argument("--rows", type=int, default=0,
+                    help="single-search workloads: the first ROWS database rows only (small profiling cases)")
+    ap.add_argument("--queries", type=int, default=0, help="single-search workloads: the first QUERIES queries only")
     ap.add_argument("--serve-n", type=int, default=5_000_000, help="serving workload: database rows")
     ap.add_argument("--serve-rates", type=lambda v: [int(x) for x in v.split(",")], default=[1000, 5000, 20000, 50000],
                     help="serving workload: offered query rates (queries/s)")
