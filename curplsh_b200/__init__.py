@@ -138,6 +138,8 @@ def _load():
         "curplsh_get_coarse_check": (i32, [ctypes.POINTER(ctypes.c_int)]),
         "curplsh_set_cta_pairs": (i32, [i32]),
         "curplsh_get_cta_pairs": (i32, [ctypes.POINTER(ctypes.c_int)]),
+        "curplsh_set_dual_blocks": (i32, [i32]),
+        "curplsh_get_dual_blocks": (i32, [ctypes.POINTER(ctypes.c_int)]),
         "curplsh_index_estimate_plan": (i32, [vp, i64, i32, i32, i32, ctypes.POINTER(ctypes.c_int),
                                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
         "curplsh_index_get_fallback_count": (i32, [vp, ctypes.POINTER(ctypes.c_int64)]),
@@ -170,7 +172,7 @@ EXPORTED_SYMBOLS = (
     "curplsh_set_bound_estimate", "curplsh_get_bound_estimate", "curplsh_index_estimate_plan",
     "curplsh_index_get_fallback_count", "curplsh_estimate_plan_shape", "curplsh_set_coarse_check",
     "curplsh_get_coarse_check", "curplsh_index_get_coarse_fallback_count", "curplsh_set_cta_pairs",
-    "curplsh_get_cta_pairs",
+    "curplsh_get_cta_pairs", "curplsh_set_dual_blocks", "curplsh_get_dual_blocks",
 )
 
 
@@ -552,6 +554,19 @@ def set_cta_pairs(enabled: bool) -> None:
 def get_cta_pairs() -> bool:
     v = ctypes.c_int(0)
     _check(_lib.curplsh_get_cta_pairs(ctypes.byref(v)))
+    return bool(v.value)
+
+
+def set_dual_blocks(enabled: bool) -> None:
+    """Process-wide switch of dual query blocks (on by default): FP8 fused passes
+    over >= 4 query blocks keep two blocks per CTA against 128-row database tiles
+    (results do not depend on it)."""
+    _check(_lib.curplsh_set_dual_blocks(1 if enabled else 0))
+
+
+def get_dual_blocks() -> bool:
+    v = ctypes.c_int(0)
+    _check(_lib.curplsh_get_dual_blocks(ctypes.byref(v)))
     return bool(v.value)
 
 

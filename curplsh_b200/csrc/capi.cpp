@@ -462,7 +462,7 @@ SearchShape search_shape(const curplsh_index* ix, int nq, int k, int form, int r
   sh.kp = kprime_for(form, k, rerank_factor, ix->n, coarse_on);
   const TuneParams tp = tune_lookup(form, ix->dim, k, nq);
   sh.P = pool_capacity(sh.kp, tp.headroom);
-  plan_fused(nq, (int)ix->n, ix->dres->num_sms, &sh.plan, default_split_q4(tp, sh.P));
+  plan_fused(nq, (int)ix->n, ix->dres->num_sms, &sh.plan, default_split_q4(tp, sh.P), form, ix->dim);
   sh.nq_pad = round_up(nq, kBM);
   sh.pool_lists = (size_t)sh.plan.pool_rows() * sh.plan.units_per_block;
   if (allow_est) sh.est = plan_estimate(nq, ix->n, sh.kp, ix->dres->num_sms);
@@ -1209,6 +1209,17 @@ int curplsh_set_cta_pairs(int enabled) {
 int curplsh_get_cta_pairs(int* enabled) {
   if (!enabled) return set_error(CURPLSH_ERR_INVALID_ARG, "null argument");
   *enabled = get_cta_pairs();
+  return CURPLSH_OK;
+}
+
+int curplsh_set_dual_blocks(int enabled) {
+  set_dual_blocks(enabled);
+  return CURPLSH_OK;
+}
+
+int curplsh_get_dual_blocks(int* enabled) {
+  if (!enabled) return set_error(CURPLSH_ERR_INVALID_ARG, "null argument");
+  *enabled = get_dual_blocks();
   return CURPLSH_OK;
 }
 

@@ -127,6 +127,8 @@ struct FusedBatch {
   int form;
   int d;                   // dimension shared by every item of the launch
   int pair;                // 1: clusters of two CTAs, one 256-row MMA over two query blocks
+  int dual;                // 1: each CTA holds two query blocks against 128-row database tiles
+  int pad1;
   long long total_work;    // sum of G_i * T_i (G_i: query groups of 128 << pair rows)
   long long work_per_cta;  // W, per CTA (per pair when pair = 1)
   uint32_t* status;        // device error word

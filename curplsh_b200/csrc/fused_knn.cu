@@ -95,15 +95,18 @@ struct SmemLayout {
   uint32_t pool_off;   // per-row candidate pool counts and bounds
   uint32_t total;      // dynamic smem bytes requested (includes 1 KB alignment slack)
   uint32_t b_chunk;    // bytes of one B part of a K chunk (this CTA's database rows)
+  uint32_t a_block;    // bytes between the two resident query blocks (dual)
   uint32_t b_tail;     // bytes of the B tail chunk
 };
 
 // pair = 1: this CTA holds half of each 256-row database tile (CTA pairs);
-// epi_warps: epilogue warps (each has a 1 KB histogram / staging area).
-__host__ __device__ inline SmemLayout make_layout(int form, int d, int pair = 0, int epi_warps = kEpiWarps) {
+// epi_warps: epilogue warps (each has a 1 KB histogram / staging area);
+// dual = 1: two resident query blocks (a_block bytes apart) and 128-row tiles.
+__host__ __device__ inline SmemLayout make_layout(int form, int d, int pair = 0, int epi_warps = kEpiWarps,
+                                                  int dual = 0) {
   SmemLayout L{};
-  L.b_chunk = pair ? kBChunkBytes / 2 : kBChunkBytes;
-  L.b_tail = pair ? kBTailBytes / 2 : kBTailBytes;
+  L.b_chunk = (pair || dual) ? kBChunkBytes / 2 : kBChunkBytes;
+  L.b_tail = (pair || dual) ? kBTailBytes / 2 : kBTailBytes;
   const bool folded = form != kFormFP8;
   const int chunk_elems = folded ? 64 : 128;
   const int a_parts = (form == kFormExact) ? 2 : 1;
@@ -114,9 +117,12 @@ __host__ __device__ inline SmemLayout make_layout(int form, int d, int pair = 0,
   // the tail runs the hi x hi product alone, which is exact only for those
   L.tail_narrow = folded && (d % 64 == 0);
   // everything below the barrier block must fit the 227 KB opt-in limit
-  const uint32_t budget = 227u * 1024u - 256u - (uint32_t)epi_warps * 256u * 4u - 1024u - 1024u;
+  const uint32_t pool_bytes = dual ? 2048u : 1024u;  // pool counts and bounds of 128 (dual: 256) rows
+  const uint32_t budget = 227u * 1024u - 256u - (uint32_t)epi_warps * 256u * 4u - pool_bytes - 1024u;
   const int nreg = L.nkc - (L.tail_narrow ? 1 : 0);
-  const uint32_t a_res = (uint32_t)nreg * a_parts * kAChunkBytes + (L.tail_narrow ? kATailBytes : 0u);
+  const uint32_t a_one = (uint32_t)nreg * a_parts * kAChunkBytes + (L.tail_narrow ? kATailBytes : 0u);
+  L.a_block = (a_one + 1023u) & ~1023u;
+  const uint32_t a_res = dual ? 2u * L.a_block : a_one;
   // a stage = one regular K chunk of the tile; the last one also carries the tail
   const uint32_t b_stage = (uint32_t)b_parts * L.b_chunk + (L.tail_narrow ? L.b_tail : 0u);
   if (((a_res + 1023u) & ~1023u) + 2 * b_stage <= budget) {
@@ -134,7 +140,7 @@ __host__ __device__ inline SmemLayout make_layout(int form, int d, int pair = 0,
   L.bar_off = L.a_bytes + (uint32_t)L.stages * L.stage_bytes;
   L.hist_off = L.bar_off + 256;  // barriers: 2*8 + 6 mbarriers + tmem slot + flags < 256 B
   L.pool_off = L.hist_off + epi_warps * 256 * 4;
-  L.total = L.pool_off + 1024 + 1024;
+  L.total = L.pool_off + pool_bytes + 1024;
   return L;
 }
 
@@ -179,8 +185,8 @@ struct UnitWalk {
   long long pos, end, W;
   int ii, shift, rank;
   __device__ UnitWalk(int cta, const FusedBatch& B, uint32_t cta_rank)
-      : W(B.work_per_cta), ii(0), shift(B.pair), rank((int)cta_rank) {
-    pos = (long long)(cta >> shift) * W;
+      : W(B.work_per_cta), ii(0), shift(B.pair | B.dual), rank((int)cta_rank) {
+    pos = (long long)(cta >> B.pair) * W;
     end = pos + W < B.total_work ? pos + W : B.total_work;
   }
   template <int MAXI>
@@ -361,8 +367,12 @@ __device__ __forceinline__ float select32(const float (&v)[32], int j) {
 // PAIR selects the CTA-pair kernel: a kernel that contains cta_group::2
 // instructions can only be launched as clusters of two, so the single-CTA
 // kernel is a separate instance without them.
-template <int FORM, int MAXI, bool MINIMA = false, bool PAIR = false>
+// DUAL: two query blocks resident per CTA; each 128-row database tile feeds two
+// 128 x 128 MMAs (one per block), so a tile crosses L2 -> SM once per 256
+// queries without coupling CTAs; warp g of a lane group filters block g.
+template <int FORM, int MAXI, bool MINIMA = false, bool PAIR = false, bool DUAL = false>
 __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const __grid_constant__ FusedArgs<MAXI> A) {
+  static_assert(!(PAIR && DUAL) && !(DUAL && MINIMA), "dual blocks: single CTAs, candidate pools");
   using Tr = FormTraits<FORM>;
   const FusedBatch& B = A.B;
   // a conditional pass (a re-search after a failed check): every thread of
@@ -373,7 +383,9 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   constexpr int EW = epi_warps_for(MINIMA);  // epilogue warps
   constexpr int WG = EW / 4;                  // epilogue warps per TMEM lane group
-  const SmemLayout L = make_layout(FORM, B.d, PAIR ? 1 : 0, EW);
+  const SmemLayout L = make_layout(FORM, B.d, PAIR ? 1 : 0, EW, DUAL ? 1 : 0);
+  constexpr int kTileRows = DUAL ? kBN / 2 : kBN;  // database rows per tile
+  constexpr int kQB = DUAL ? 2 : 1;                // resident query blocks
   const int S = L.stages;
   // CTA pairs: rank 0 issues the MMAs and owns the barriers the pair's loads
   // complete on; each CTA loads and filters its own query block
@@ -472,19 +484,24 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
           }
           const int nreg = L.nkc - (L.tail_narrow ? 1 : 0);
           if (issuer)
-            mbar_arrive_expect_tx(a_full, tx_mul * ((uint32_t)nreg * Tr::kAParts * kAChunkBytes +
-                                                    (L.tail_narrow ? kATailBytes : 0u)));
-          for (int kc = 0; kc < nreg; ++kc)
-            for (int part = 0; part < Tr::kAParts; ++part)
-              load(smem + a_res_off(L, kc, part, Tr::kAParts), part ? &tm_q_lo : &tm_q_hi, a_full, kc * KC, qb * kBM,
-                   pol_q);
-          if (L.tail_narrow)
-            load(smem + a_res_off(L, nreg, 0, Tr::kAParts), &tm_q_tail, a_full, nreg * KC, qb * kBM, pol_q);
+            mbar_arrive_expect_tx(a_full, tx_mul * (uint32_t)kQB *
+                                              ((uint32_t)nreg * Tr::kAParts * kAChunkBytes +
+                                               (L.tail_narrow ? kATailBytes : 0u)));
+          for (int j = 0; j < kQB; ++j) {
+            uint8_t* ab = smem + (uint32_t)j * L.a_block;
+            const int qrow = (qb + j) * kBM;
+            for (int kc = 0; kc < nreg; ++kc)
+              for (int part = 0; part < Tr::kAParts; ++part)
+                load(ab + a_res_off(L, kc, part, Tr::kAParts), part ? &tm_q_lo : &tm_q_hi, a_full, kc * KC, qrow,
+                     pol_q);
+            if (L.tail_narrow)
+              load(ab + a_res_off(L, nreg, 0, Tr::kAParts), &tm_q_tail, a_full, nreg * KC, qrow, pol_q);
+          }
         }
         const int nreg = L.nkc - (L.tail_narrow ? 1 : 0);
         for (int t = t0; t < t1 && ok; ++t) {
           const int T_i = A.items[ii].num_tiles;
-          const int tx_row = ((t - rot + T_i) % T_i) * kBN + half_row;  // database tile of position t
+          const int tx_row = ((t - rot + T_i) % T_i) * kTileRows + half_row;  // database tile of position t
           for (int kc = 0; kc < nreg; ++kc, ++it) {
             const int s = (int)(it % (uint32_t)S);
             STAT_BEGIN(tw);
@@ -521,7 +538,7 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
     if (lane == 0 && issuer) {
       constexpr uint32_t fmt = Tr::kFP8 ? 0u : 1u;  // e4m3 : bf16
       // a pair's MMA is 256 rows: this CTA's query block, then the partner's
-      const uint32_t idesc = make_idesc(fmt, fmt, pair ? 2 * kBM : kBM, kBN);
+      const uint32_t idesc = make_idesc(fmt, fmt, pair ? 2 * kBM : kBM, DUAL ? kBN / 2 : kBN);
       auto mma = [&](uint32_t d_tmem, uint64_t ad, uint64_t bd, uint32_t acc, bool f8) {
         if constexpr (PAIR) {
           if (f8)
@@ -583,24 +600,33 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
             const uint32_t st = smem_u32(smem + L.a_bytes + (uint32_t)s * L.stage_bytes);
             const int rem = L.kdim - kc * KC;
             const int nsteps = rem >= KC ? KC / Tr::kStepElems : (rem + Tr::kStepElems - 1) / Tr::kStepElems;
+            for (int j = 0; j < kQB; ++j) {  // dual: block j accumulates into columns j * 128 of the slot
+              uint32_t acc_j = accumulate;
 #pragma unroll
-            for (int pr = 0; pr < Tr::kProducts; ++pr) {
-              const uint32_t a_addr = L.a_stream ? st + stage_a_off<Tr::kAParts, Tr::kBParts>(L, Tr::a_part(pr))
-                                                 : smem_u32(smem + a_res_off(L, kc, Tr::a_part(pr), Tr::kAParts));
-              const uint32_t b_addr = st + Tr::b_part(pr) * L.b_chunk;
-              for (int ks = 0; ks < nsteps; ++ks) {
-                const uint64_t ad = sw128_kmajor_desc(a_addr + ks * 32);
-                const uint64_t bd = sw128_kmajor_desc(b_addr + ks * 32);
-                mma(d_tmem, ad, bd, accumulate, Tr::kFP8);
-                accumulate = 1;
+              for (int pr = 0; pr < Tr::kProducts; ++pr) {
+                const uint32_t a_addr =
+                    L.a_stream ? st + stage_a_off<Tr::kAParts, Tr::kBParts>(L, Tr::a_part(pr))
+                               : smem_u32(smem + (uint32_t)j * L.a_block + a_res_off(L, kc, Tr::a_part(pr), Tr::kAParts));
+                const uint32_t b_addr = st + Tr::b_part(pr) * L.b_chunk;
+                for (int ks = 0; ks < nsteps; ++ks) {
+                  const uint64_t ad = sw128_kmajor_desc(a_addr + ks * 32);
+                  const uint64_t bd = sw128_kmajor_desc(b_addr + ks * 32);
+                  mma(d_tmem + (uint32_t)j * (kBN / 2), ad, bd, acc_j, Tr::kFP8);
+                  acc_j = 1;
+                }
               }
             }
+            accumulate = 1;
             if (L.tail_narrow && kc == nreg - 1) {
               // the 16 norm columns: only hi x hi carries them (lo rows are zero
               // there), so one K step of product 0 with the 32-byte-swizzled tiles
               const uint32_t tl = st + stage_tail_off<Tr::kAParts, Tr::kBParts>(L);
-              const uint32_t a_addr = L.a_stream ? tl + L.b_tail : smem_u32(smem + a_res_off(L, nreg, 0, Tr::kAParts));
-              mma(d_tmem, sw32_kmajor_desc(a_addr), sw32_kmajor_desc(tl), 1, false);
+              for (int j = 0; j < kQB; ++j) {
+                const uint32_t a_addr =
+                    L.a_stream ? tl + L.b_tail
+                               : smem_u32(smem + (uint32_t)j * L.a_block + a_res_off(L, nreg, 0, Tr::kAParts));
+                mma(d_tmem + (uint32_t)j * (kBN / 2), sw32_kmajor_desc(a_addr), sw32_kmajor_desc(tl), 1, false);
+              }
             }
             commit(&empty[s]);
           }
@@ -639,8 +665,8 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
     const int pair_bar = 1 + lg;   // named barrier of the WG warps of lane group lg
     constexpr int kGroupThreads = 32 * WG;
     uint32_t* hist = hist_all + ew * 256;
-    int* cnt_s = reinterpret_cast<int*>(smem + L.pool_off);             // [128] pool counts
-    float* thr_s = reinterpret_cast<float*>(smem + L.pool_off) + kBM;   // [128] pool bounds
+    int* cnt_s = reinterpret_cast<int*>(smem + L.pool_off);                   // [128 kQB] pool counts
+    float* thr_s = reinterpret_cast<float*>(smem + L.pool_off) + kQB * kBM;   // [128 kQB] pool bounds
     const uint32_t lane_base = (uint32_t)(lg * 32) << 16;
     UnitWalk walk(blockIdx.x, B, rank);
     int ii, qb, t0, t1, u_ord, rot;
@@ -668,7 +694,10 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
         raise_abort(abort_flag, B.status, kErrBadSchedule);
         break;
       }
-      const int q = qb * kBM + row;
+      // dual: warp g filters query block qb + g and owns its pools alone
+      const int qbw = DUAL ? qb + g : qb;
+      const int crow = DUAL ? g * kBM + row : row;  // this lane's pool count / bound slot
+      const int q = qbw * kBM + row;
       const bool valid = q < p.nq;
       const float qn = valid ? p.q_norms[q] : 0.f;
       float m2s = -2.f;
@@ -676,18 +705,21 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
       // FP8 with one scale s for every database row: d = ||x||^2 + (-2 s_q s) acc
       const bool uniform = Tr::kFP8 && p.db_scale_uniform > 0.f;
       const float ku = m2s * p.db_scale_uniform;
-      const size_t pool_row0 = (size_t)qb * kBM;  // pool index of lane-group row 0 is added per lane
+      const size_t pool_row0 = (size_t)qbw * kBM;  // pool index of lane-group row 0 is added per lane
       auto pool_of = [&](int r) -> uint64_t* {
         return p.pools + ((pool_row0 + (size_t)r) * U + (size_t)u_ord) * (size_t)P;
       };
       uint64_t* pool = pool_of(row);
       // a new unit starts with an empty pool (the previous unit's last barrier
       // ordered every use of the old state before this)
-      if (g == 0) {
-        cnt_s[row] = 0;
-        thr_s[row] = 3.402823466e38f;
+      if (DUAL || g == 0) {
+        cnt_s[crow] = 0;
+        thr_s[crow] = 3.402823466e38f;
       }
-      bar_sync_named(pair_bar, kGroupThreads);
+      if constexpr (DUAL)
+        __syncwarp();
+      else
+        bar_sync_named(pair_bar, kGroupThreads);
       float thr = 3.402823466e38f;  // FLT_MAX: admits every finite distance until a pool fills
 
       // Selections of the pools in `need` (lane bits of this lane group; warp g
@@ -702,13 +734,14 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
           need &= need - 1;
           STAT_INC(st_nref, 1);
           const int r = lg * 32 + src;
-          const int n_src = cnt_s[r];
+          const int cr = (DUAL ? g * kBM : 0) + r;
+          const int n_src = cnt_s[cr];
           int kept = 0;
           const uint64_t kmax = warp_select_keep_any(pool_of(r), n_src < P ? n_src : P, keep, P, hist, kept);
           if (lane == src) {
             const uint32_t ord = (uint32_t)(kmax >> 32);
-            cnt_s[r] = kept;
-            thr_s[r] = fminf(thr_s[r], thr_from<Tr::kFolded>(ord2f(ord), qn));
+            cnt_s[cr] = kept;
+            thr_s[cr] = fminf(thr_s[cr], thr_from<Tr::kFolded>(ord2f(ord), qn));
             // only a full set of k' keys bounds the global k'-th distance
             if (kept >= p.kprime) atomicMin(&p.q_bound[q], ord);
           }
@@ -722,7 +755,7 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
       for (int t = t0; t < t1; ++t, ++tc) {
         const uint32_t slot = tc & 1u, use = tc >> 1;
         const int tphys = (t - rot + p.num_tiles) % p.num_tiles;  // database tile of position t
-        thr = fminf(thr, thr_s[row]);
+        thr = fminf(thr, thr_s[crow]);
         if (nb_ob != kOrdInf) thr = fminf(thr, thr_from<Tr::kFolded>(ord2f(nb_ob), qn));
         const float thr_up = next_above(thr);  // d <= thr  <=>  d < thr_up
         if (valid) nb_ob = ld_relaxed_u32(&p.q_bound[q]);
@@ -746,7 +779,7 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
           for (int i = 0; i < 4; ++i) {
             const int cc = my_c[i >> 1] < 0 ? my_c[0] : my_c[i >> 1];
             // < nb_pad: rows are padded to whole tiles (a strided sample has no padding)
-            const int c0 = tphys * kBN + cc * 64 + lane + 32 * (i & 1);
+            const int c0 = tphys * kTileRows + (DUAL ? cc - 2 * g : cc) * 64 + lane + 32 * (i & 1);
             const size_t c = MINIMA ? (size_t)c0 * (size_t)p.db_step : (size_t)c0;
             pxn[i] = __ldg(p.db_norms + c);
             psx[i] = uniform ? 0.f : __ldg(p.db_scale + c);
@@ -780,7 +813,7 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
           tmem_ld_32x32b_x64(tmem_base + lane_base + slot * kBN + ch * 64, v);
           tmem_ld_wait();
           STAT_END(ttm, st_tmem);
-          const int col0 = tphys * kBN + ch * 64;
+          const int col0 = tphys * kTileRows + (DUAL ? ch - 2 * g : ch) * 64;
           // coarse distances of the 64 columns (two independent 32-column halves)
           float da[32], db[32];
           if (Tr::kFolded) {
@@ -877,7 +910,7 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
             // slots for this lane's survivors of the 64 columns, reserved at
             // once by every lane (most add 0): no branch, so the select trees
             // below run while the shared atomic is in flight
-            int n = atomicAdd(&cnt_s[row], __popc(ma) + __popc(mb));
+            int n = atomicAdd(&cnt_s[crow], __popc(ma) + __popc(mb));
             if ((ma & mb) == ~0u) {
               // every column survives (a pool with no bound yet): append all
               // 64 keys in column order, no extraction
@@ -944,7 +977,11 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
         // together if either aborted
         if ((t - t0 + 1) % S != 0 && t + 1 < t1) continue;
         STAT_BEGIN(tb1);
-        const bool leave = bar_red_or(pair_bar, kGroupThreads, !got || *abort_flag != 0);
+        bool leave;
+        if constexpr (DUAL)
+          leave = __any_sync(0xffffffffu, !got || *abort_flag != 0);
+        else
+          leave = bar_red_or(pair_bar, kGroupThreads, !got || *abort_flag != 0);
         STAT_END(tb1, st_bar);
         if (leave) {
           ok = false;
@@ -953,24 +990,30 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
         // pools that may not have room for the next S tiles (both halves),
         // or, at the unit's end, every pool above k' (the merge pass reads at
         // most k' keys' worth beyond what it needs)
-        const int lim = t + 1 < t1 ? P - S * kBN : p.kprime;
-        const bool mine = (lane % WG) == g;
-        const int cn = mine ? cnt_s[row] : 0;
+        const int lim = t + 1 < t1 ? P - S * kTileRows : p.kprime;
+        const bool mine = DUAL || (lane % WG) == g;
+        const int cn = mine ? cnt_s[crow] : 0;
         if (cn > P) atomicOr(B.status, kErrPoolOverflow);
         refresh(__ballot_sync(0xffffffffu, mine && valid && cn > lim), p.kprime);
         STAT_BEGIN(tb2);
-        bar_sync_named(pair_bar, kGroupThreads);
+        if constexpr (DUAL)
+          __syncwarp();
+        else
+          bar_sync_named(pair_bar, kGroupThreads);
         STAT_END(tb2, st_bar);
       }
       if (!ok) break;
       // a refresh may keep a few more than k' keys (unsorted): record them all;
       // the merge pass selects exactly
-      if (!MINIMA && valid && g == 0) {
-        const int cn = cnt_s[row];
+      if (!MINIMA && valid && (DUAL || g == 0)) {
+        const int cn = cnt_s[crow];
         p.pool_counts[(pool_row0 + row) * U + u_ord] = cn < P ? cn : P;
         if (gap) p.pool_counts[(pool_row0 + row) * U + u_ord - 1] = 0;
       }
-      bar_sync_named(pair_bar, kGroupThreads);  // the counts are read before the next unit resets them
+      if constexpr (DUAL)
+        __syncwarp();
+      else
+        bar_sync_named(pair_bar, kGroupThreads);  // the counts are read before the next unit resets them
     }
     if (lane == 0) {
       STAT_FLUSH(kStatEpiWaitAccFull, st_wait);
@@ -1043,13 +1086,14 @@ bool make_map(CUtensorMap* m, const void* base, bool fp8, long long rows, long l
 }
 
 // Raises the kernel's dynamic shared memory limit once per device.
-template <int FORM, int MAXI, bool MINIMA = false, bool PAIR = false>
+template <int FORM, int MAXI, bool MINIMA = false, bool PAIR = false, bool DUAL = false>
 cudaError_t ensure_attributes() {
   static bool attr_done[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr_done[dev & 63]) {
-    cudaError_t e = cudaFuncSetAttribute(fused_knn_kernel<FORM, MAXI, MINIMA, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(fused_knn_kernel<FORM, MAXI, MINIMA, PAIR, DUAL>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          227 * 1024);
     if (e != cudaSuccess) return e;
     attr_done[dev & 63] = true;
@@ -1057,13 +1101,13 @@ cudaError_t ensure_attributes() {
   return cudaSuccess;
 }
 
-template <int FORM, int MAXI, bool MINIMA = false, bool PAIR = false>
+template <int FORM, int MAXI, bool MINIMA = false, bool PAIR = false, bool DUAL = false>
 cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, int n, const FusedBatchPlan& bp,
                         uint32_t* status, unsigned long long* stats, uint32_t smem, cudaStream_t st,
                         const int* run_if) {
-  cudaError_t e = ensure_attributes<FORM, MAXI, MINIMA, PAIR>();
+  cudaError_t e = ensure_attributes<FORM, MAXI, MINIMA, PAIR, DUAL>();
   if (e != cudaSuccess) return e;
-  smem = make_layout(FORM, specs[0].d, PAIR ? 1 : 0, epi_warps_for(MINIMA)).total;  // this instance's layout
+  smem = make_layout(FORM, specs[0].d, PAIR ? 1 : 0, epi_warps_for(MINIMA), DUAL ? 1 : 0).total;  // this instance's
   FusedArgs<MAXI> a;
   memset(&a, 0, sizeof(a));
   a.B.num_items = n;
@@ -1072,7 +1116,8 @@ cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, 
   a.B.pair = bp.pair;
   a.B.total_work = bp.total_work;
   a.B.work_per_cta = bp.work_per_cta;
-  const int xrows = kBN >> bp.pair;  // database rows one CTA loads per tile
+  a.B.dual = bp.dual;
+  const int xrows = kBN >> (bp.pair | bp.dual);  // database rows one CTA loads per tile
   a.B.status = status;
   a.B.stats = stats;
   a.B.run_if = run_if;
@@ -1127,7 +1172,7 @@ cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, 
     }
   }
   if (!PAIR) {
-    fused_knn_kernel<FORM, MAXI, MINIMA, PAIR><<<bp.grid, threads_for(MINIMA), smem, st>>>(a);
+    fused_knn_kernel<FORM, MAXI, MINIMA, PAIR, DUAL><<<bp.grid, threads_for(MINIMA), smem, st>>>(a);
     return cudaGetLastError();
   }
   if (bp.grid % 2) return cudaErrorInvalidValue;
@@ -1143,7 +1188,7 @@ cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, 
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, fused_knn_kernel<FORM, MAXI, MINIMA, PAIR>, a);
+  return cudaLaunchKernelEx(&cfg, fused_knn_kernel<FORM, MAXI, MINIMA, PAIR, DUAL>, a);
 }
 
 template <int FORM>
@@ -1155,6 +1200,14 @@ cudaError_t launch_form_any(const FusedItemSpec* specs, const FusedItemPlan* pla
                    : launch_form<FORM, 1, true>(specs, plans, n, bp, status, stats, smem, st, run_if);
   for (int i = 0; i < n; ++i)
     if (specs[i].minima) return cudaErrorInvalidValue;  // block-minimum mode is single-item
+  if constexpr (FORM != kFormExact) {
+    if (bp.dual)
+      return n == 1 ? launch_form<FORM, 1, false, false, true>(specs, plans, n, bp, status, stats, smem, st, run_if)
+                    : launch_form<FORM, kFusedMaxItems, false, false, true>(specs, plans, n, bp, status, stats, smem,
+                                                                          st, run_if);
+  } else {
+    if (bp.dual) return cudaErrorInvalidValue;  // dual blocks are planned for BF16 / FP8 only
+  }
   if (n == 1)
     return bp.pair ? launch_form<FORM, 1, false, true>(specs, plans, n, bp, status, stats, smem, st, run_if)
                    : launch_form<FORM, 1>(specs, plans, n, bp, status, stats, smem, st, run_if);
@@ -1164,41 +1217,59 @@ cudaError_t launch_form_any(const FusedItemSpec* specs, const FusedItemPlan* pla
 
 }  // namespace
 
+#ifndef CURPLSH_DUAL_DEFAULT
+#define CURPLSH_DUAL_DEFAULT 1
+#endif
 namespace {
 std::atomic<int> g_cta_pairs{0};
+std::atomic<int> g_dual{CURPLSH_DUAL_DEFAULT};
 }  // namespace
 
 void set_cta_pairs(int on) { g_cta_pairs.store(on ? 1 : 0, std::memory_order_relaxed); }
 int get_cta_pairs() { return g_cta_pairs.load(std::memory_order_relaxed); }
+void set_dual_blocks(int on) { g_dual.store(on ? 1 : 0, std::memory_order_relaxed); }
+int get_dual_blocks() { return g_dual.load(std::memory_order_relaxed); }
 
-void plan_fused_batch(const FusedItemSpec* specs, int n, int max_ctas, FusedItemPlan* plans, FusedBatchPlan* out) {
-  // CTA pairs when there are enough query blocks and few groups of two would
-  // be half empty (an item with an odd block count leaves one CTA of its last
-  // group without queries)
+void plan_fused_batch(const FusedItemSpec* specs, int n, int max_ctas, FusedItemPlan* plans, FusedBatchPlan* out,
+                      int form) {
+  // Query groups of two blocks (dual blocks in one CTA for BF16/FP8, else CTA
+  // pairs when on) when there are enough query blocks and few groups would be
+  // half empty (an item with an odd block count leaves its last group one
+  // block short)
   long long blocks = 0, odd = 0;
   for (int i = 0; i < n; ++i) {
     const long long g = specs[i].nb > 0 ? (specs[i].nq + kBM - 1) / kBM : 0;
     blocks += g;
     odd += g & 1;
   }
-  const int pair = (get_cta_pairs() && max_ctas >= 2 && blocks >= 4 && odd * 8 <= blocks) ? 1 : 0;
-  const int rows = kBM << pair;
+  const bool grouped = blocks >= 4 && odd * 8 <= blocks;
+  // dual blocks need both query blocks resident in shared memory
+  const bool dual_fits = n > 0 && specs[0].d > 0 && !make_layout(form, specs[0].d, 0, kPoolEpiWarps, 1).a_stream;
+  // FP8 only: its MMAs are light, so halving the tile bytes per query pays
+  // (sphere 39.6 -> 37.7 ms); the BF16 pass got slower (3.50 -> 4.52 ms on the
+  // integer mixture: twice the MMA instructions and shared-memory A reads)
+  const int dual = (grouped && dual_fits && get_dual_blocks() && form == kFormFP8) ? 1 : 0;
+  const int pair = (!dual && grouped && get_cta_pairs() && max_ctas >= 2) ? 1 : 0;
+  const int rows = kBM << (pair | dual);
+  const int tile_rows = dual ? kBN / 2 : kBN;
   long long total = 0;
   for (int i = 0; i < n; ++i) {
     FusedItemPlan& pl = plans[i];
     pl.num_qblocks = specs[i].nb > 0 ? (specs[i].nq + rows - 1) / rows : 0;
-    pl.num_tiles = (specs[i].nb + kBN - 1) / kBN;
+    pl.num_tiles = (specs[i].nb + tile_rows - 1) / tile_rows;
     pl.split_tiles = specs[i].split_tiles > 0 && specs[i].split_tiles < pl.num_tiles ? specs[i].split_tiles
                                                                                       : std::max(pl.num_tiles, 1);
     pl.work_begin = total;
     total += (long long)pl.num_qblocks * pl.num_tiles;
     pl.work_end = total;
     pl.pair = pair;
+    pl.dual = dual;
   }
   const long long units = max_ctas >> pair;  // CTAs, or pairs of CTAs
   long long grid = units < total ? units : total;
   if (grid < 1) grid = 1;
   out->pair = pair;
+  out->dual = dual;
   out->total_work = total;
   out->work_per_cta = total > 0 ? (total + grid - 1) / grid : 1;
   out->grid = total > 0 ? (int)((total + out->work_per_cta - 1) / out->work_per_cta) << pair : 0;
@@ -1215,22 +1286,24 @@ void plan_fused_batch(const FusedItemSpec* specs, int n, int max_ctas, FusedItem
   }
 }
 
-void plan_fused(int nq, int nb, int num_sms, FusedPlan* out, int split_q4) {
+void plan_fused(int nq, int nb, int num_sms, FusedPlan* out, int split_q4, int form, int d) {
   FusedItemSpec s{};
   s.nq = nq;
   s.nb = nb;
+  s.d = d;
   FusedItemPlan ip;
   FusedBatchPlan bp;
-  plan_fused_batch(&s, 1, num_sms, &ip, &bp);
+  plan_fused_batch(&s, 1, num_sms, &ip, &bp, form);
   if (split_q4 < 4 && bp.grid > 0) {
     s.split_tiles = split_tiles_for(bp.work_per_cta, split_q4);
-    plan_fused_batch(&s, 1, num_sms, &ip, &bp);
+    plan_fused_batch(&s, 1, num_sms, &ip, &bp, form);
   }
   out->num_qblocks = ip.num_qblocks;
   out->num_tiles = ip.num_tiles;
   out->work_per_cta = bp.work_per_cta;
   out->grid = bp.grid;
   out->pair = bp.pair;
+  out->dual = bp.dual;
   out->units_per_block = ip.units_per_block;
   out->split_tiles = ip.split_tiles;
 }
@@ -1253,6 +1326,8 @@ cudaError_t prepare_fused_kernels(int form) {
       if (e == cudaSuccess) e = ensure_attributes<kFormBF16, 1, false, true>();
       if (e == cudaSuccess) e = ensure_attributes<kFormBF16, 1, true, true>();
       if (e == cudaSuccess) e = ensure_attributes<kFormBF16, kFusedMaxItems, false, true>();
+      if (e == cudaSuccess) e = ensure_attributes<kFormBF16, 1, false, false, true>();
+      if (e == cudaSuccess) e = ensure_attributes<kFormBF16, kFusedMaxItems, false, false, true>();
       return e != cudaSuccess ? e : ensure_attributes<kFormBF16, kFusedMaxItems>();
     case kFormFP8:
       e = ensure_attributes<kFormFP8, 1>();
@@ -1260,6 +1335,8 @@ cudaError_t prepare_fused_kernels(int form) {
       if (e == cudaSuccess) e = ensure_attributes<kFormFP8, 1, false, true>();
       if (e == cudaSuccess) e = ensure_attributes<kFormFP8, 1, true, true>();
       if (e == cudaSuccess) e = ensure_attributes<kFormFP8, kFusedMaxItems, false, true>();
+      if (e == cudaSuccess) e = ensure_attributes<kFormFP8, 1, false, false, true>();
+      if (e == cudaSuccess) e = ensure_attributes<kFormFP8, kFusedMaxItems, false, false, true>();
       return e != cudaSuccess ? e : ensure_attributes<kFormFP8, kFusedMaxItems>();
     default:
       return cudaErrorInvalidValue;
@@ -1322,11 +1399,13 @@ cudaError_t launch_fused(const FusedLaunch& f, cudaStream_t st) {
   ip.work_begin = 0;
   ip.work_end = (long long)f.plan.num_qblocks * f.plan.num_tiles;
   ip.pair = f.plan.pair;
+  ip.dual = f.plan.dual;
   FusedBatchPlan bp;
   bp.total_work = ip.work_end;
   bp.work_per_cta = f.plan.work_per_cta;
   bp.grid = f.plan.grid;
   bp.pair = f.plan.pair;
+  bp.dual = f.plan.dual;
   return launch_fused_batch(f.form, &s, &ip, 1, bp, f.status, f.stats, st, f.run_if);
 }
 

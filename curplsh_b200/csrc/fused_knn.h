@@ -15,8 +15,9 @@ struct FusedPlan {
   int units_per_block = 0;    // U: max units (pool lists) of one query block
   int split_tiles = 1;        // L: resolved unit length limit
   int pair = 0;               // 1: clusters of two CTAs share each 256-row MMA (two query blocks)
+  int dual = 0;               // 1: one CTA holds two query blocks against 128-row database tiles
   // pool rows of the plan (pools and counts are indexed by query row)
-  long long pool_rows() const { return (long long)num_qblocks * (128LL << pair); }
+  long long pool_rows() const { return (long long)num_qblocks * (128LL << (pair | dual)); }
 };
 
 // Tuned launch parameters for one (form, d, k, Q) bucket (tuning.cpp).
@@ -73,7 +74,8 @@ struct FusedLaunch {
 
 // One search over at most num_sms CTAs.  split_q4 < 4 cuts units shorter than
 // the CTA ranges (split_tiles_for(W, split_q4)); >= 4 leaves the ranges whole.
-void plan_fused(int nq, int nb, int num_sms, FusedPlan* out, int split_q4 = 4);
+// `form` (-1: unknown) decides whether dual blocks may be used (BF16 and FP8).
+void plan_fused(int nq, int nb, int num_sms, FusedPlan* out, int split_q4 = 4, int form = -1, int d = 0);
 uint32_t fused_smem_bytes(int form, int d);
 cudaError_t launch_fused(const FusedLaunch& f, cudaStream_t st);
 
@@ -110,19 +112,25 @@ struct FusedItemPlan {
   int split_tiles;  // resolved split length L (>= 1)
   long long work_begin, work_end;
   int pair;         // the launch's FusedBatchPlan::pair
+  int dual;         // the launch's FusedBatchPlan::dual
 };
 struct FusedBatchPlan {
   long long total_work = 0, work_per_cta = 1;
   int grid = 0;
   int pair = 0;  // 1: clusters of two CTAs; work_per_cta is per pair and grid counts CTAs
+  int dual = 0;  // 1: each CTA takes query groups of two blocks and 128-row database tiles
 };
-// CTA pairs on (1, default) or off for the plans made after the call.
+// CTA pairs on (1) or off (0, default) for the plans made after the call.
 void set_cta_pairs(int on);
 int get_cta_pairs();
+// Dual query blocks (BF16 / FP8) on or off for the plans made after the call.
+void set_dual_blocks(int on);
+int get_dual_blocks();
 // Plans `n` items over at most `max_ctas` CTAs.  Only nq, nb and split_tiles
 // of the specs are read, so pool sizes (which depend on units_per_block) can be computed
 // from the plan before the pools are carved.
-void plan_fused_batch(const FusedItemSpec* specs, int n, int max_ctas, FusedItemPlan* plans, FusedBatchPlan* out);
+void plan_fused_batch(const FusedItemSpec* specs, int n, int max_ctas, FusedItemPlan* plans, FusedBatchPlan* out,
+                      int form = -1);
 // Sets the kernels' launch attributes on the current device (done lazily by
 // the launches; call it before a stream capture).
 cudaError_t prepare_fused_kernels(int form);

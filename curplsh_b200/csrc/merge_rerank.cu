@@ -473,7 +473,7 @@ cudaError_t launch_merge_rerank(const MergeLaunch& m, cudaStream_t st) {
   it.pool_cap = m.pool_cap;
   it.num_tiles = m.plan.num_tiles;
   it.units_per_block = m.plan.units_per_block;
-  it.pair = m.plan.pair;
+  it.pair = m.plan.pair | m.plan.dual;
   it.row0 = 0;
   it.split_tiles = m.plan.split_tiles > 0 ? m.plan.split_tiles : 1;
   it.work_begin = 0;

@@ -130,6 +130,7 @@ int MultiPlan::build(const curplsh_batch_item* items, int n, const std::vector<c
         const FItem& x = fitems_[FL.fitems[j]];
         specs[j].nq = x.nq;
         specs[j].nb = (int)views[x.slot].n;
+        specs[j].d = G.d;
         // units as long as the item's own CTA ranges would be if it were
         // searched alone (scaled by the tuned split, at most the whole range,
         // as alone), so its in-pool selection work stays what it is alone
@@ -137,7 +138,7 @@ int MultiPlan::build(const curplsh_batch_item* items, int n, const std::vector<c
         specs[j].split_tiles = split_tiles_for(std::max<long long>(1, (own + num_sms - 1) / num_sms),
                                                std::min(default_split_q4(x.tune, x.P), 4));
       }
-      plan_fused_batch(specs.data(), (int)specs.size(), num_sms, plans.data(), &FL.bp);
+      plan_fused_batch(specs.data(), (int)specs.size(), num_sms, plans.data(), &FL.bp, G.form);
       for (size_t j = 0; j < FL.fitems.size(); ++j) {
         FItem& x = fitems_[FL.fitems[j]];
         x.plan = plans[j];
@@ -182,7 +183,8 @@ int MultiPlan::build(const curplsh_batch_item* items, int n, const std::vector<c
     x.o_bounds = o_bounds_ + bcur * sizeof(uint32_t);
     bcur += (size_t)x.nq_pad;
     if (v.n == 0) continue;
-    const size_t lists = (size_t)x.plan.num_qblocks * ((size_t)kBM << x.plan.pair) * x.plan.units_per_block;
+    const size_t lists = (size_t)x.plan.num_qblocks * ((size_t)kBM << (x.plan.pair | x.plan.dual)) *
+                         x.plan.units_per_block;
     if (x.form != kFormFP8) x.o_qh = take((size_t)x.nq_pad * v.ld16 * 2);
     if (x.form == kFormExact) x.o_ql = take((size_t)x.nq_pad * v.ld16 * 2);
     if (x.form == kFormFP8) x.o_q8 = take((size_t)x.nq_pad * v.ld8);
@@ -366,7 +368,7 @@ int MultiPlan::enqueue(cudaStream_t main, const std::vector<cudaStream_t>* branc
           m.pool_cap = x.P;
           m.num_tiles = v.n > 0 ? x.plan.num_tiles : 0;
           m.units_per_block = v.n > 0 ? x.plan.units_per_block : 1;
-          m.pair = x.plan.pair;
+          m.pair = x.plan.pair | x.plan.dual;
           m.row0 = x.row0[j];
           m.split_tiles = v.n > 0 ? x.plan.split_tiles : 1;
           m.work_begin = x.plan.work_begin;

@@ -152,7 +152,7 @@ int search_noalloc_locked(const IndexView& v, int nq, const float* q, int k, int
   Layout L{};
   int cap = v.num_sms;
   for (;;) {
-    plan_fused(nq, (int)v.n, cap, &plan);
+    plan_fused(nq, (int)v.n, cap, &plan, 4, form, v.dim);
     const size_t lists = (size_t)plan.pool_rows() * plan.units_per_block;
     L = carve(form, nq_pad, v.ld16, v.ld8, lists, P);
     if (L.total <= kNoAllocScratchBytes || cap == 1) break;

@@ -333,6 +333,12 @@ int curplsh_get_coarse_check(int* enabled);
  * Applies to searches, batches and servers planned after the call.  Process-wide. */
 int curplsh_set_cta_pairs(int enabled);
 int curplsh_get_cta_pairs(int* enabled);
+/* Dual query blocks (engine-specific, no counterpart in cuRPLSH; on by default): an FP8 fused
+ * pass over at least four 128-query blocks keeps two blocks resident in each CTA and feeds each
+ * 128-row database tile to two 128 x 128 tensor-core MMAs, so a tile crosses from L2 once per 256
+ * queries.  Results do not depend on it.  Applies to plans made after the call; process-wide. */
+int curplsh_set_dual_blocks(int enabled);
+int curplsh_get_dual_blocks(int* enabled);
 /* Number of queries this index searched again in the exact form after their coarse margin
  * failed (since creation). */
 int curplsh_index_get_coarse_fallback_count(curplsh_index* index, int64_t* count);
