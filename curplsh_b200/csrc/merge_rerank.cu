@@ -26,16 +26,13 @@ namespace curplsh_b200 {
 
 namespace {
 
-// Threads per query's CTA (a build option: 256 or 128); the radix histogram has
-// 256 bins, 256 / kMergeThreads per thread.  128 threads put twice as many
-// queries in flight per SM at the same register budget (merge of a 10^4-query
-// BF16 search 0.32 -> 0.28 ms).
-#ifndef CURPLSH_MERGE_THREADS
-#define CURPLSH_MERGE_THREADS 128
-#endif
-constexpr int kMergeThreads = CURPLSH_MERGE_THREADS;
-static_assert(kMergeThreads == 256 || kMergeThreads == 128, "256 or 128 merge threads");
-constexpr int kBinsPerThread = 256 / kMergeThreads;
+// Threads per query's CTA: 128 or 256, chosen per launch (the radix histogram
+// has 256 bins, 256 / threads per thread).  128-thread CTAs put twice as many
+// queries in flight per SM at the same register budget and win where a
+// query's rerank is small (k' x d <= 65536: merge of a 10^4-query BF16 search
+// at k' = 224, d = 128, 0.32 -> 0.28 ms); 256 win where it is large (the
+// batched workload, d up to 512: 93 -> 74 ms per graph replay).
+constexpr int kMergeSmallRerank = 65536;
 // Candidates one warp reranks at once: each lane keeps this many database rows
 // in flight (a row of d = 128 is one 16-byte load per lane).
 #ifndef CURPLSH_RERANK_ROWS
@@ -73,7 +70,7 @@ struct MergeArgs {
 // visited by `each` are <= B (keys are unique).  `each(f)` calls f(key) for
 // every key of this thread's share.  8-bit digits from the top; stops as soon
 // as the digit bucket holds exactly the remaining rank.
-template <class Each>
+template <int T, class Each>
 __device__ uint64_t block_select_bound(Each each, uint32_t keep, uint32_t* hist, uint32_t* warp_tot,
                                        uint32_t* misc) {
   const int tid = threadIdx.x;
@@ -81,24 +78,24 @@ __device__ uint64_t block_select_bound(Each each, uint32_t keep, uint32_t* hist,
   uint32_t rank = keep;
   for (int shift = 56; shift >= 0; shift -= 8) {
 #pragma unroll
-    for (int b = 0; b < kBinsPerThread; ++b) hist[tid * kBinsPerThread + b] = 0u;
+    for (int b = 0; b < (256 / T); ++b) hist[tid * (256 / T) + b] = 0u;
     __syncthreads();
     each([&](uint64_t key) {
       if ((key & pmask) == prefix) atomicAdd(&hist[(uint32_t)(key >> shift) & 255u], 1u);
     });
     __syncthreads();
-    uint32_t cb[kBinsPerThread], c = 0;
+    uint32_t cb[(256 / T)], c = 0;
 #pragma unroll
-    for (int b = 0; b < kBinsPerThread; ++b) {
-      cb[b] = hist[tid * kBinsPerThread + b];
+    for (int b = 0; b < (256 / T); ++b) {
+      cb[b] = hist[tid * (256 / T) + b];
       c += cb[b];
     }
     const uint32_t incl = block_incl_scan(c, warp_tot);
     uint32_t excl = incl - c;
 #pragma unroll
-    for (int b = 0; b < kBinsPerThread; ++b) {
+    for (int b = 0; b < (256 / T); ++b) {
       if (excl < rank && rank <= excl + cb[b]) {
-        misc[1] = (uint32_t)(tid * kBinsPerThread + b);
+        misc[1] = (uint32_t)(tid * (256 / T) + b);
         misc[2] = excl;
         misc[3] = cb[b];
       }
@@ -121,11 +118,8 @@ __device__ uint64_t block_select_bound(Each each, uint32_t keep, uint32_t* hist,
 // SM); at 6 CTAs (40 registers, a few spills) the merge of a 10^4-query search
 // dropped from 0.62 to 0.32 ms (BF16, k' = 224).  12 for 128 threads: the same
 // 40-register budget.
-#ifndef CURPLSH_MERGE_MIN_BLOCKS
-#define CURPLSH_MERGE_MIN_BLOCKS (kMergeThreads == 128 ? 12 : 6)
-#endif
-__global__ void __launch_bounds__(kMergeThreads, CURPLSH_MERGE_MIN_BLOCKS)
-    merge_rerank_kernel(const __grid_constant__ MergeArgs a) {
+template <int NT>
+__global__ void __launch_bounds__(NT, NT == 128 ? 12 : 6) merge_rerank_kernel(const __grid_constant__ MergeArgs a) {
   if (a.run_if && *a.run_if == 0) return;  // a conditional re-merge whose check passed
   int lo = 0, hi = a.num_items - 1;  // last item with q_begin <= blockIdx.x
   while (lo < hi) {
@@ -165,7 +159,7 @@ __global__ void __launch_bounds__(kMergeThreads, CURPLSH_MERGE_MIN_BLOCKS)
   uint32_t qbound = 0xFFFFFFFFu;
   if (m.q_bound && T > 0 && a.pre_cap > 0) qbound = m.q_bound[prow];
 
-  for (int i = tid; i < d; i += kMergeThreads) qv[i] = m.queries[(size_t)q * d + i];
+  for (int i = tid; i < d; i += NT) qv[i] = m.queries[(size_t)q * d + i];
   if (tid == 0) {
     misc[0] = 0;
     misc[4] = 0;
@@ -173,13 +167,13 @@ __global__ void __launch_bounds__(kMergeThreads, CURPLSH_MERGE_MIN_BLOCKS)
     misc[6] = 0xFFFFFFFFu;   // min of the same
     misc[7] = 0u;            // largest coarse distance among the candidates, order bits
   }
-  for (int l = tid; l < nlists; l += kMergeThreads) lcnt[l] = m.pool_counts[list0 + l];
+  for (int l = tid; l < nlists; l += NT) lcnt[l] = m.pool_counts[list0 + l];
   __syncthreads();
   auto list_ptr = [&](int l) { return m.pools + (list0 + (size_t)l) * (size_t)m.pool_cap; };
   auto each_pool_key = [&](auto f) {
     for (int l = 0; l < nlists; ++l) {
       const uint64_t* lp = list_ptr(l);
-      for (int o = tid; o < lcnt[l]; o += kMergeThreads) {
+      for (int o = tid; o < lcnt[l]; o += NT) {
         const uint64_t key = lp[o];
         if ((uint32_t)(key >> 32) <= qbound) f(key);
       }
@@ -214,16 +208,16 @@ __global__ void __launch_bounds__(kMergeThreads, CURPLSH_MERGE_MIN_BLOCKS)
   uint64_t bound = ~0ull;
   if (cnt > keep) {
     if (cnt <= a.pre_cap)
-      bound = block_select_bound(
+      bound = block_select_bound<NT>(
           [&](auto f) {
-            for (int i = tid; i < cnt; i += kMergeThreads) f(pre[i]);
+            for (int i = tid; i < cnt; i += NT) f(pre[i]);
           },
           (uint32_t)keep, hist, warp_tot, misc);
     else
-      bound = block_select_bound(each_pool_key, (uint32_t)keep, hist, warp_tot, misc);
+      bound = block_select_bound<NT>(each_pool_key, (uint32_t)keep, hist, warp_tot, misc);
   }
   if (cnt <= a.pre_cap) {
-    for (int i = tid; i < cnt; i += kMergeThreads) {
+    for (int i = tid; i < cnt; i += NT) {
       const uint64_t key = pre[i];
       if (key <= bound) {
         const uint32_t pos = atomicAdd(&misc[4], 1u);
@@ -248,7 +242,7 @@ __global__ void __launch_bounds__(kMergeThreads, CURPLSH_MERGE_MIN_BLOCKS)
   // (that many rows in flight per lane), lane-strided partial sums then a
   // butterfly, in the same fixed order for every row
   constexpr int R = kRerankRows;
-  for (int c = R * warp; c < kept; c += R * (kMergeThreads / 32)) {
+  for (int c = R * warp; c < kept; c += R * (NT / 32)) {
     uint32_t ii[R];
     float s[R];
 #pragma unroll
@@ -343,14 +337,14 @@ __global__ void __launch_bounds__(kMergeThreads, CURPLSH_MERGE_MIN_BLOCKS)
       }
     }
   }
-  for (int c = kept + tid; c < a.kp2; c += kMergeThreads) cand[c] = kKeyEmpty;
+  for (int c = kept + tid; c < a.kp2; c += NT) cand[c] = kKeyEmpty;
   __syncthreads();
   // ---- 4. bitonic sort by (exact distance, row)
   int n2 = 1;
   while (n2 < kept) n2 <<= 1;
   for (int size = 2; size <= n2; size <<= 1) {
     for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      for (int i = tid; i < n2 / 2; i += kMergeThreads) {
+      for (int i = tid; i < n2 / 2; i += NT) {
         const int lo2 = 2 * i - (i & (stride - 1));
         const int hi2 = lo2 + stride;
         const bool asc = (lo2 & size) == 0;
@@ -388,7 +382,7 @@ __global__ void __launch_bounds__(kMergeThreads, CURPLSH_MERGE_MIN_BLOCKS)
       if (m.coarse_count) atomicAdd(m.coarse_count, 1);
     }
   }
-  for (int t = tid; t < m.k; t += kMergeThreads) {
+  for (int t = tid; t < m.k; t += NT) {
     int oi = -1;
     float od = 3.402823466e38f;
     if (t < kept) {
@@ -409,7 +403,9 @@ cudaError_t prepare_merge_kernel() {
   cudaGetDevice(&dev);
   if (!attr_done[dev & 63]) {
     cudaError_t e =
-        cudaFuncSetAttribute(merge_rerank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaFuncSetAttribute(merge_rerank_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(merge_rerank_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     if (e != cudaSuccess) return e;
     attr_done[dev & 63] = true;
   }
@@ -460,7 +456,10 @@ cudaError_t launch_merge_batch(MergeItem* items, int n, int d, uint32_t* status,
   cudaError_t e = prepare_merge_kernel();
   if (e != cudaSuccess) return e;
   if (smem > 200 * 1024 || qsum > 0x7fffffffLL) return cudaErrorInvalidValue;
-  merge_rerank_kernel<<<(unsigned)qsum, kMergeThreads, smem, st>>>(a);
+  if ((long long)kpmax * d <= kMergeSmallRerank)
+    merge_rerank_kernel<128><<<(unsigned)qsum, 128, smem, st>>>(a);
+  else
+    merge_rerank_kernel<256><<<(unsigned)qsum, 256, smem, st>>>(a);
   return cudaGetLastError();
 }
 
