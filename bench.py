@@ -389,7 +389,7 @@ def run_single(cb, synth, wl, args, world, rank, local, res, peaks, fp8_peak, wi
         "workload": wl, "value": Q * world / (ms / 1e3), "ms_per_step": ms,
         "dtype": FORMS[headline].split("_")[0], "data": info["data"],
         "config": {"workload": wl, "N": n_db, "Q": Q, "d": dim, "k": k, "form": FORMS[headline],
-                   "kprime": {"bf16_rerank": "2k (coarse-margin check on)", "fp8_rerank": "max(4k, 320)", "fp32_exact": "k + 16", "rounding": "up to a multiple of 32"}, "l2": info["l2"], "seed": synth.SEEDS[wl],
+                   "kprime": {"bf16_rerank": "2k (coarse-margin check on)", "fp8_rerank": "max(4k, 480)", "fp32_exact": "k + 16", "rounding": "up to a multiple of 32"}, "l2": info["l2"], "seed": synth.SEEDS[wl],
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "recall_at_k": rec, "recall_ok": rec is not None and rec >= 1.0,
         "forms": forms_out,

@@ -18,6 +18,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <shared_mutex>
 #include <string>
 #include <vector>
 
@@ -195,6 +196,7 @@ int init_device(curplsh_resources* r, int device, DevRes** out) {
 // ------------------------------------------------------------------ index
 namespace {
 struct StreamWorkspace {
+  std::mutex mu;   // held for a whole search on this stream (callers sharing a stream take turns)
   DevBuf dev;      // query operands, pools, staging
   DevBuf fb;       // re-search of the queries an estimated bound failed
   PinnedBuf host;  // status read-back
@@ -214,7 +216,11 @@ struct curplsh_index {
   int dim = 0;
   curplsh_bf_config cfg{};
   DevRes* dres = nullptr;
-  std::mutex mu;
+  // Searches hold `mu` shared (they run concurrently, each on its own stream's
+  // workspace); add, reset and destroy hold it exclusively.
+  std::shared_mutex mu;
+  std::mutex ws_mu;   // the stream -> workspace map
+  std::mutex fp8_mu;  // building the FP8 copy on first use
   // database
   int64_t n = 0;
   long long n_pad = 0;
@@ -272,6 +278,7 @@ constexpr float kFP8UniformSpan = 16.f;
 
 int build_fp8(curplsh_index* ix, cudaStream_t st) {
   if (ix->n == 0) return CURPLSH_OK;
+  std::lock_guard<std::mutex> lk(ix->fp8_mu);  // concurrent searches build it once
   if (!ix->x8) {
     CUDA_TRY(cudaMalloc(&ix->x8, (size_t)ix->n_pad * ix->ld8));
     CUDA_TRY(cudaMalloc(&ix->xs, (size_t)ix->n_pad * sizeof(float)));
@@ -306,14 +313,15 @@ int build_fp8(curplsh_index* ix, cudaStream_t st) {
 // short of a true neighbour and the check listed none; k' = k listed 1.7% of
 // the uniform queries.  Unverified searches (batch graph, serving loop,
 // allocation-free entry) keep the wider 4k margin.
-// FP8: 4k and at least 320, verified or not.  E4M3's coarse error (~2% of a
+// FP8: 4k and at least 480, verified or not.  E4M3's coarse error (~2% of a
 // distance) needs a wider margin than BF16's (~0.4%): on the 10M-row
 // unit-sphere mixture (k = 10), k' = 40 left 19 of 10,000 FP8 queries short of
-// a true neighbour and the check sent 78% of them to the exact form; at
-// k' = 320 none was short and it sent 0.2%.  A fixed factor of 32 instead
-// would make k' = 3200 at k = 100, where pools that large cost ten times the
-// pass.
-constexpr long long kFP8MinCandidates = 320;
+// a true neighbour and the check sent 78% of them to the exact form; from
+// k' = 320 up none was short, and the check sent 174 queries at 320, 36 at
+// 416, 17 at 480, 1 at 640 (searches 42.8, 41.8, 41.7, 42.4 ms with the
+// re-searches).  A fixed factor instead would make k' = 4800 at k = 100,
+// where pools that large cost many times the pass.
+constexpr long long kFP8MinCandidates = 480;
 
 int kprime_for(int form, int k, int rerank_factor, int64_t n, bool checked) {
   long long kp;
@@ -724,7 +732,7 @@ int do_search(curplsh_index* ix, int64_t num, const float* queries, int k, int p
   const int form = precision < 0 ? ix->cfg.precision : precision;
   if (form < 0 || form > 2) return set_error(CURPLSH_ERR_INVALID_ARG, "unknown precision %d", precision);
   const int rf = rerank_factor > 0 ? rerank_factor : ix->cfg.rerank_factor;
-  std::lock_guard<std::mutex> lk(ix->mu);
+  std::shared_lock<std::shared_mutex> lk(ix->mu);
   DeviceScope scope(ix->cfg.device);
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ix->dres->def;
   if (!stream) {
@@ -756,9 +764,15 @@ int do_search(curplsh_index* ix, int64_t num, const float* queries, int k, int p
   const bool dev_recheck = est && !coarse && all_dev && !force_sync;
   const bool sync = force_sync || (est && !dev_recheck) || coarse || !all_dev;
 
-  auto& slot = ix->ws[st];
-  if (!slot) slot.reset(new StreamWorkspace());
-  StreamWorkspace& w = *slot;
+  StreamWorkspace* wp;
+  {
+    std::lock_guard<std::mutex> wl(ix->ws_mu);
+    auto& slot = ix->ws[st];
+    if (!slot) slot.reset(new StreamWorkspace());
+    wp = slot.get();
+  }
+  StreamWorkspace& w = *wp;
+  std::lock_guard<std::mutex> wlk(w.mu);
   const size_t core = search_workspace_bytes(ix, nq, k, form, rf, est, coarse);
   const size_t qbytes = q_dev ? 0 : (size_t)nq * ix->dim * sizeof(float);
   const size_t obytes = (i_dev && d_dev) ? 0 : (size_t)nq * k * (sizeof(int) + sizeof(float));
@@ -852,7 +866,7 @@ int do_search(curplsh_index* ix, int64_t num, const float* queries, int k, int p
 namespace curplsh_b200 {
 int index_lock_view(curplsh_index* ix, IndexView* v) {
   if (!ix || !v) return set_error(CURPLSH_ERR_INVALID_ARG, "null argument");
-  ix->mu.lock();
+  ix->mu.lock_shared();
   v->device = ix->cfg.device;
   v->dim = ix->dim;
   v->precision = ix->cfg.precision;
@@ -875,7 +889,7 @@ int index_lock_view(curplsh_index* ix, IndexView* v) {
   v->fp8_ready = ix->fp8_ev;
   return CURPLSH_OK;
 }
-void index_unlock(curplsh_index* ix) { ix->mu.unlock(); }
+void index_unlock(curplsh_index* ix) { ix->mu.unlock_shared(); }
 int index_prepare_form(curplsh_index* ix, int form, IndexView* v) {
   if (form != kFormFP8 || ix->x8 || ix->n == 0) return CURPLSH_OK;
   DeviceScope scope(ix->cfg.device);
@@ -1077,7 +1091,7 @@ int curplsh_index_add(curplsh_index* ix, int64_t num, const float* data) {
   if (!data) return set_error(CURPLSH_ERR_INVALID_ARG, "null data");
   if (ix->n + num > ((int64_t)1 << 31) - 1024)
     return set_error(CURPLSH_ERR_UNSUPPORTED, "more than 2^31 - 1024 rows in one index");
-  std::lock_guard<std::mutex> lk(ix->mu);
+  std::unique_lock<std::shared_mutex> lk(ix->mu);
   DeviceScope scope(ix->cfg.device);
   cudaStream_t st = ix->dres->def;
   const int d = ix->dim;
@@ -1158,7 +1172,7 @@ int curplsh_index_search_profiled(curplsh_index* ix, int64_t num, const float* q
 
 int curplsh_index_reset(curplsh_index* ix) {
   if (!ix) return set_error(CURPLSH_ERR_INVALID_ARG, "null index");
-  std::lock_guard<std::mutex> lk(ix->mu);
+  std::unique_lock<std::shared_mutex> lk(ix->mu);
   DeviceScope scope(ix->cfg.device);
   cudaStreamSynchronize(ix->dres->def);
   for (auto& kv : ix->ws) cudaStreamSynchronize(kv.first);
@@ -1231,7 +1245,7 @@ int curplsh_index_estimate_plan(curplsh_index* ix, int64_t num, int k, int preci
   const int form = precision < 0 ? ix->cfg.precision : precision;
   if (form < 0 || form > 2) return set_error(CURPLSH_ERR_INVALID_ARG, "unknown precision %d", precision);
   const int rf = rerank_factor > 0 ? rerank_factor : ix->cfg.rerank_factor;
-  std::lock_guard<std::mutex> lk(ix->mu);
+  std::shared_lock<std::shared_mutex> lk(ix->mu);
   *sample_rows = 0;
   *step = 1;
   *rank = 0;

@@ -21,7 +21,7 @@ struct IndexBFConfig : public IndexConfig {
   /// coarse form: CURPLSH_PRECISION_FP32_EXACT / _BF16_RERANK / _FP8_RERANK
   int precision;
   /// k' = rerankFactor * k candidates for the BF16 / FP8 forms (0: the form's default -- BF16 2k
-  /// when the coarse-margin check is on, else 4k; FP8 4k and at least 320)
+  /// when the coarse-margin check is on, else 4k; FP8 4k and at least 480)
   int rerankFactor;
   /// keep a reference to device rows passed to add() instead of copying them
   bool borrowDeviceData;

@@ -62,7 +62,7 @@ typedef struct curplsh_bf_config {
   int32_t precision;               /* CURPLSH_PRECISION_* default for search */
   int32_t rerank_factor;           /* k' = rerank_factor * k for the BF16/FP8 forms; 0 (default): BF16
                                       2k when the coarse-margin check verifies the search, else 4k;
-                                      FP8 4k and at least 320 (E4M3's coarse error needs the margin) */
+                                      FP8 4k and at least 480 (E4M3's coarse error needs the margin) */
   int32_t borrow_device_data;      /* 1: add() of device memory keeps a reference to the caller's FP32
                                       rows (the reference's aliasing, include/device_tensor.h:97-103);
                                       0 (default): the index copies them */
