@@ -563,8 +563,15 @@ def run_serving(cb, synth, args, world, rank, local, res):
     import numpy as np
     import torch
 
+    import gc
+
     import oracle
     dev = f"cuda:{local}"
+    # free what earlier workloads left to the garbage collector now: freeing a
+    # pinned host buffer (cudaFreeHost) takes the driver for tens of ms, and a
+    # collection during a latency measurement shows up as one slow request
+    gc.collect()
+    torch.cuda.empty_cache()
     n, d, k = args.serve_n, 256, 50
     base, qpool = synth.mixture_bf16(n, 20000, d, seed=synth.SEEDS["serving"], backend="torch", device=dev)
     torch.cuda.synchronize()
@@ -638,6 +645,7 @@ def run_serving(cb, synth, args, world, rank, local, res):
             arrivals = np.cumsum(gaps) - gaps[0]
             # a slower sampler with a longer settle: each nvidia-smi query takes
             # driver locks that a latency measurement would otherwise see
+            gc.collect()
             sampler = ClockSampler(local, interval_ms=200, settle_s=1.0)
             sampler.__enter__()
             lat, wall, (_, _, ph) = run_load(srv, sizes, list(arrivals))
