@@ -648,7 +648,11 @@ def run_serving(cb, synth, args, world, rank, local, res):
             gc.collect()
             sampler = ClockSampler(local, interval_ms=200, settle_s=1.0)
             sampler.__enter__()
-            lat, wall, (_, _, ph) = run_load(srv, sizes, list(arrivals))
+            gc.disable()
+            try:
+                lat, wall, (_, _, ph) = run_load(srv, sizes, list(arrivals))
+            finally:
+                gc.enable()
             sampler.__exit__(None, None, None)
             sm = [float(x.split(",")[0]) for x in sampler.lines if x and x.split(",")[0].strip().replace(".", "").isdigit()]
             slow = np.argsort(-lat)[:3]
