@@ -567,11 +567,22 @@ def run_serving(cb, synth, args, world, rank, local, res):
 
     import oracle
     dev = f"cuda:{local}"
-    # free what earlier workloads left to the garbage collector now: freeing a
-    # pinned host buffer (cudaFreeHost) takes the driver for tens of ms, and a
-    # collection during a latency measurement shows up as one slow request
+    # free what earlier workloads left to the garbage collector now, and run
+    # no collection during the measurements: freeing a pinned host buffer
+    # (cudaFreeHost) takes the driver for milliseconds, and a collection inside
+    # a timed load shows up as one slow request or a slower saturated run
     gc.collect()
     torch.cuda.empty_cache()
+    gc.disable()
+    try:
+        return _serving_measure(cb, synth, args, rank, local, res, oracle, dev)
+    finally:
+        gc.enable()
+
+
+def _serving_measure(cb, synth, args, rank, local, res, oracle, dev):
+    import numpy as np
+    import torch
     n, d, k = args.serve_n, 256, 50
     base, qpool = synth.mixture_bf16(n, 20000, d, seed=synth.SEEDS["serving"], backend="torch", device=dev)
     torch.cuda.synchronize()
@@ -645,14 +656,9 @@ def run_serving(cb, synth, args, world, rank, local, res):
             arrivals = np.cumsum(gaps) - gaps[0]
             # a slower sampler with a longer settle: each nvidia-smi query takes
             # driver locks that a latency measurement would otherwise see
-            gc.collect()
             sampler = ClockSampler(local, interval_ms=200, settle_s=1.0)
             sampler.__enter__()
-            gc.disable()
-            try:
-                lat, wall, (_, _, ph) = run_load(srv, sizes, list(arrivals))
-            finally:
-                gc.enable()
+            lat, wall, (_, _, ph) = run_load(srv, sizes, list(arrivals))
             sampler.__exit__(None, None, None)
             sm = [float(x.split(",")[0]) for x in sampler.lines if x and x.split(",")[0].strip().replace(".", "").isdigit()]
             slow = np.argsort(-lat)[:3]

@@ -295,7 +295,7 @@ int build_fp8(curplsh_index* ix, cudaStream_t st) {
       memcpy(&hi, &range[1], sizeof(float));
       if (hi <= kFP8UniformSpan * lo) {
         CUDA_TRY(launch_prep_rows(ix->x32, ix->dim, (int)ix->n, ix->n_pad, ix->dim, nullptr, 0.f, nullptr, nullptr,
-                                  ix->ld16, ix->x8, ix->xs, ix->ld8, st, kAugNone, nullptr, hi));
+                                  ix->ld16, ix->x8, ix->xs, ix->ld8, st, kAugF8Database, nullptr, hi));
         ix->xs_uniform = hi;
       }
     }
@@ -574,7 +574,7 @@ int search_device(curplsh_index* ix, int nq, const float* q_dev, int k, int form
 
   tm->rec(1, st);
   CUDA_TRY(launch_prep_rows(q_dev, d, nq, nq_pad, d, b.qn, 0.f, form == kFormFP8 ? nullptr : b.qh, b.ql, ix->ld16,
-                            b.q8, b.qs, ix->ld8, st, form == kFormFP8 ? kAugNone : kAugQuery));
+                            b.q8, b.qs, ix->ld8, st, form == kFormFP8 ? kAugF8Query : kAugQuery));
   FusedLaunch f{};
   f.nq = nq;
   f.nb = (int)ix->n;
@@ -1040,7 +1040,9 @@ int curplsh_index_bf_create(curplsh_resources* r, int dim, const curplsh_bf_conf
   ix->cfg = c;
   ix->dres = d;
   ix->ld16 = round_up(dim + kAugCols, 8);  // BF16 rows carry the augmented norm columns
-  ix->ld8 = round_up(dim, 16);
+  // FP8 rows: the codes, then, when round_up(d, 32) leaves 32 bytes of the
+  // last 128-byte K chunk free, the BF16 norm tail there
+  ix->ld8 = (round_up(dim, 32) % 128 != 0) ? round_up(dim, 32) + 32 : round_up(dim, 16);
   r->refs.fetch_add(1);
   DeviceScope scope(c.device);
   cudaError_t e = cudaMalloc(&ix->status, 6 * sizeof(uint32_t));

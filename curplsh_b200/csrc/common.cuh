@@ -114,6 +114,12 @@ struct FusedItem {
   uint32_t* q_bound;       // [nq_pad] shared per-query bound (ordered bits), init kOrdInf or an estimate
   int db_step;             // database row j of this item is stored row j * db_step (>= 1)
   float db_scale_uniform;  // > 0: every database row has this FP8 scale (db_scale is not read)
+  // FP8 form with one database scale s: > 0 is the byte offset of the 32-byte
+  // BF16 norm tail of the FP8 rows (query rows [a_h a_h a_l], a = 1/s_q;
+  // database rows [b_h b_l b_h], b = -||x||^2 / (2 s)).  One K=16 BF16 MMA over
+  // the tails adds ||x||^2 / (-2 s_q s) to the FP8 accumulator, which then is
+  // (||x||^2 - 2 q.x) / (-2 s_q s): no database norm is loaded per tile.
+  int fp8_tail;
   // Non-null: block-minimum mode (no pools): minima[q * 2 * num_tiles + 2 * t + h]
   // gets the smallest key distance of query q over rows [256 t + 128 h, +128).
   float* minima;

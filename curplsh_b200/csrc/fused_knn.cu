@@ -299,11 +299,12 @@ __device__ __forceinline__ uint32_t shl1_sign(uint32_t acc, uint32_t t) {
   asm("shf.l.wrap.b32 %0, %1, %2, 1;" : "=r"(r) : "r"(t), "r"(acc));
   return r;
 }
-// bit j set iff dv[j] < u (u = next_above(thr): dv[j] <= thr)
-__device__ __forceinline__ uint32_t survive_mask32(const float (&dv)[32], float u) {
+// bit j set iff km dv[j] < u, computed exactly (one rounding of km dv[j] - u
+// keeps its sign); u = next_above(thr) makes it km dv[j] <= thr for km = 1
+__device__ __forceinline__ uint32_t survive_mask32(const float (&dv)[32], float km, float u) {
   float t[32];
 #pragma unroll
-  for (int i = 0; i < 16; ++i) fma2_f32(t[2 * i], t[2 * i + 1], dv[2 * i], dv[2 * i + 1], 1.f, 1.f, -u, -u);
+  for (int i = 0; i < 16; ++i) fma2_f32(t[2 * i], t[2 * i + 1], dv[2 * i], dv[2 * i + 1], km, km, -u, -u);
   uint32_t c[8];
 #pragma unroll
   for (int p = 0; p < 8; ++p) {
@@ -539,17 +540,20 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
       constexpr uint32_t fmt = Tr::kFP8 ? 0u : 1u;  // e4m3 : bf16
       // a pair's MMA is 256 rows: this CTA's query block, then the partner's
       const uint32_t idesc = make_idesc(fmt, fmt, pair ? 2 * kBM : kBM, DUAL ? kBN / 2 : kBN);
+      // the FP8 form's BF16 norm tail: the same shape, BF16 operands
+      const uint32_t idesc16 = make_idesc(1u, 1u, pair ? 2 * kBM : kBM, DUAL ? kBN / 2 : kBN);
       auto mma = [&](uint32_t d_tmem, uint64_t ad, uint64_t bd, uint32_t acc, bool f8) {
+        const uint32_t id = f8 ? idesc : idesc16;
         if constexpr (PAIR) {
           if (f8)
-            mma_f8_ss_pair(d_tmem, ad, bd, idesc, acc);
+            mma_f8_ss_pair(d_tmem, ad, bd, id, acc);
           else
-            mma_f16_ss_pair(d_tmem, ad, bd, idesc, acc);
+            mma_f16_ss_pair(d_tmem, ad, bd, id, acc);
         } else {
           if (f8)
-            mma_f8_ss(d_tmem, ad, bd, idesc, acc);
+            mma_f8_ss(d_tmem, ad, bd, id, acc);
           else
-            mma_f16_ss(d_tmem, ad, bd, idesc, acc);
+            mma_f16_ss(d_tmem, ad, bd, id, acc);
         }
       };
       // completion goes to the barrier at the same offset in both CTAs of a pair
@@ -587,6 +591,7 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
           const uint32_t d_tmem = tmem_base + slot * kBN;
           uint32_t accumulate = 0;
           const int nreg = L.nkc - (L.tail_narrow ? 1 : 0);
+          const int fp8_tail = Tr::kFP8 ? A.items[ii].fp8_tail : 0;
           for (int kc = 0; kc < nreg; ++kc, ++it) {
             const int s = (int)(it % (uint32_t)S);
             STAT_BEGIN(tf);
@@ -617,6 +622,19 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
               }
             }
             accumulate = 1;
+            if (Tr::kFP8 && fp8_tail > 0 && kc == nreg - 1) {
+              // the BF16 norm tails: one K=16 step at their byte offset in the
+              // last chunk (a 32-byte K step of the 128-byte swizzled rows, as
+              // the FP8 steps before it), into the same FP32 accumulator
+              const uint32_t toff = (uint32_t)(fp8_tail - kc * KC);
+              for (int j = 0; j < kQB; ++j) {
+                const uint32_t a_addr =
+                    L.a_stream ? st + stage_a_off<Tr::kAParts, Tr::kBParts>(L, 0)
+                               : smem_u32(smem + (uint32_t)j * L.a_block + a_res_off(L, kc, 0, Tr::kAParts));
+                mma(d_tmem + (uint32_t)j * (kBN / 2), sw128_kmajor_desc(a_addr + toff), sw128_kmajor_desc(st + toff), 1,
+                    false);
+              }
+            }
             if (L.tail_narrow && kc == nreg - 1) {
               // the 16 norm columns: only hi x hi carries them (lo rows are zero
               // there), so one K step of product 0 with the 32-byte-swizzled tiles
@@ -705,6 +723,12 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
       // FP8 with one scale s for every database row: d = ||x||^2 + (-2 s_q s) acc
       const bool uniform = Tr::kFP8 && p.db_scale_uniform > 0.f;
       const float ku = m2s * p.db_scale_uniform;
+      // with the norm tails the accumulator is d / ku: the filter compares
+      // ku acc with the bound and scales only the survivors (km = 1: the
+      // accumulator is d itself or is made d below)
+      const bool fold = Tr::kFP8 && p.fp8_tail > 0;
+      const float km = fold ? ku : 1.f;
+      auto key_d = [&](float x) -> float { return Tr::kFolded ? x : fmaf(km, x, qn); };
       const size_t pool_row0 = (size_t)qbw * kBM;  // pool index of lane-group row 0 is added per lane
       auto pool_of = [&](int r) -> uint64_t* {
         return p.pools + ((pool_row0 + (size_t)r) * U + (size_t)u_ord) * (size_t)P;
@@ -774,7 +798,7 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
         // the accumulator wait (their latency overlaps it) and staged in the
         // warp's histogram area, which is free outside a refresh
         float pxn[4], psx[4];
-        if (Tr::kFP8) {
+        if (Tr::kFP8 && !fold) {
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
             const int cc = my_c[i >> 1] < 0 ? my_c[0] : my_c[i >> 1];
@@ -795,7 +819,7 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
         tc_fence_after();
         float bmin = 3.402823466e38f;  // block-minimum mode: smallest distance of this half tile
         float* colv = reinterpret_cast<float*>(hist);  // [128] norms, then [128] scales
-        if (Tr::kFP8) {
+        if (Tr::kFP8 && !fold) {
           __syncwarp();
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
@@ -816,12 +840,20 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
           const int col0 = tphys * kTileRows + (DUAL ? ch - 2 * g : ch) * 64;
           // coarse distances of the 64 columns (two independent 32-column halves)
           float da[32], db[32];
-          if (Tr::kFolded) {
-            // the accumulator already is ||q||^2 + ||x||^2 - 2 q.x
+          if (Tr::kFolded || fold) {
+            // the accumulator already is ||q||^2 + ||x||^2 - 2 q.x (BF16 and
+            // exact forms) or (||x||^2 - 2 q.x) / ku (FP8 with norm tails)
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
               da[j] = __uint_as_float(v[j]);
               db[j] = __uint_as_float(v[32 + j]);
+            }
+            if (MINIMA && fold) {
+#pragma unroll
+              for (int j = 0; j < 32; j += 2) {
+                mul2_f32(da[j], da[j + 1], da[j], da[j + 1], ku, ku);
+                mul2_f32(db[j], db[j + 1], db[j], db[j + 1], ku, ku);
+              }
             }
           } else {
             const float4* xn4 = reinterpret_cast<const float4*>(colv + h * 64);
@@ -884,8 +916,8 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
             ma = survive_mask32_cmp(da, thr);
             mb = survive_mask32_cmp(db, thr);
           } else {
-            ma = survive_mask32(da, thr_up);
-            mb = survive_mask32(db, thr_up);
+            ma = survive_mask32(da, km, thr_up);
+            mb = survive_mask32(db, km, thr_up);
           }
           if (!valid) ma = mb = 0u;
           // database rows beyond nb (padding of the last tile) never survive
@@ -916,11 +948,11 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
               // 64 keys in column order, no extraction
 #pragma unroll
               for (int j = 0; j < 32; ++j)
-                if (n + j < P) pool[n + j] = make_key(Tr::kFolded ? da[j] : da[j] + qn, (uint32_t)(col0 + j));
+                if (n + j < P) pool[n + j] = make_key(key_d(da[j]), (uint32_t)(col0 + j));
 #pragma unroll
               for (int j = 0; j < 32; ++j)
                 if (n + 32 + j < P)
-                  pool[n + 32 + j] = make_key(Tr::kFolded ? db[j] : db[j] + qn, (uint32_t)(col0 + 32 + j));
+                  pool[n + 32 + j] = make_key(key_d(db[j]), (uint32_t)(col0 + 32 + j));
               n += 64;
               ma = mb = 0u;
               STAT_INC(st_surv, 64);
@@ -932,9 +964,9 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
               ma &= ma - 1u;
               mb &= mb - 1u;
               const bool ha = ja >= 0, hb = jb >= 0;
-              if (ha && n < P) pool[n] = make_key(Tr::kFolded ? xa : xa + qn, (uint32_t)(col0 + ja));
+              if (ha && n < P) pool[n] = make_key(key_d(xa), (uint32_t)(col0 + ja));
               n += ha ? 1 : 0;
-              if (hb && n < P) pool[n] = make_key(Tr::kFolded ? xb : xb + qn, (uint32_t)(col0 + 32 + jb));
+              if (hb && n < P) pool[n] = make_key(key_d(xb), (uint32_t)(col0 + 32 + jb));
               n += hb ? 1 : 0;
               STAT_INC(st_surv, (ha ? 1 : 0) + (hb ? 1 : 0));
             };
@@ -952,7 +984,7 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
                 while (mm) {
                   const int j = __ffsll((long long)mm) - 1;
                   mm &= mm - 1;
-                  if (n < P) pool[n] = make_key(Tr::kFolded ? stash[j] : stash[j] + qn, (uint32_t)(col0 + j));
+                  if (n < P) pool[n] = make_key(key_d(stash[j]), (uint32_t)(col0 + j));
                   ++n;
                   STAT_INC(st_surv, 1);
                 }
@@ -1145,6 +1177,7 @@ cudaError_t launch_form(const FusedItemSpec* specs, const FusedItemPlan* plans, 
     it.q_bound = f.q_bound;
     it.db_step = f.db_step > 1 ? f.db_step : 1;
     it.db_scale_uniform = f.xs_uniform;
+    it.fp8_tail = (fp8 && f.xs_uniform > 0.f) ? (int)fp8_tail_offset(f.d, f.ld8) : 0;
     it.minima = f.minima;
     CUtensorMap* m = &a.maps[i * kMapsPerItem];
     const void* qh = fp8 ? (const void*)f.q8 : (const void*)f.qh;

@@ -163,8 +163,18 @@ bool bound_estimate_enabled();
 // norm `pad_norm`.  Any of the output pointers may be null.  `aug` selects the
 // augmented BF16 row layout (kAugNone / kAugDatabase / kAugQuery, see kAugCols):
 // database rows get [n1 n2 n3 1 1 1] after column d, query rows are stored as -2q
-// followed by [1 1 1 m1 m2 m3]; lo rows get zeros there.
-enum AugMode : int { kAugNone = 0, kAugDatabase = 1, kAugQuery = 2 };
+// followed by [1 1 1 m1 m2 m3]; lo rows get zeros there.  kAugF8Query /
+// kAugF8Database write the FP8 rows' BF16 norm tail (see fp8_tail_offset):
+// query rows [a_h a_h a_l] with a = 1/s_q (a zero row takes scale 1), database
+// rows [b_h b_l b_h] with b = -||x||^2 / (2 fixed_scale) (zeros without a
+// fixed scale).
+enum AugMode : int { kAugNone = 0, kAugDatabase = 1, kAugQuery = 2, kAugF8Query = 3, kAugF8Database = 4 };
+// Byte offset of the FP8 rows' 32-byte BF16 norm tail, round_up(d, 32), when
+// a row of stride ld8 has room for it inside its last 128-byte K chunk; else 0.
+__host__ __device__ inline long long fp8_tail_offset(long long d, long long ld8) {
+  const long long t8 = (d + 31) / 32 * 32;
+  return (t8 % 128 != 0 && t8 + 32 <= ld8) ? t8 : 0;
+}
 // `lo_nonzero` (optional) gets a nonzero value when some real row element is
 // not exactly representable in BF16 (its lo part is nonzero).
 cudaError_t launch_prep_rows(const float* x, long long ldx, int nrows, long long nrows_pad, int d, float* norms,

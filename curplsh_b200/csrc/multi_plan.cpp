@@ -250,7 +250,7 @@ int MultiPlan::enqueue(cudaStream_t main, const std::vector<cudaStream_t>* branc
     std::vector<PrepSegment> segs;
     auto flush_prep = [&]() -> int {
       if (segs.empty()) return CURPLSH_OK;
-      const int aug = G.form == kFormFP8 ? kAugNone : kAugQuery;
+      const int aug = G.form == kFormFP8 ? kAugF8Query : kAugQuery;
       MP_TRY(launch_prep_segments(segs.data(), (int)segs.size(), G.d, G.ld16, G.ld8, 0.f, aug, st));
       ++kernels;
       segs.clear();

@@ -191,7 +191,7 @@ int search_noalloc_locked(const IndexView& v, int nq, const float* q, int k, int
   NA_TRY(cudaMemsetAsync(status, 0, sizeof(uint32_t), st));
   NA_TRY(cudaMemsetAsync(qbound, 0xFF, (size_t)nq_pad * sizeof(uint32_t), st));
   NA_TRY(launch_prep_rows(q, v.dim, nq, nq_pad, v.dim, qn, 0.f, form == kFormFP8 ? nullptr : qh, ql, v.ld16, q8,
-                          qs, v.ld8, st, form == kFormFP8 ? kAugNone : kAugQuery));
+                          qs, v.ld8, st, form == kFormFP8 ? kAugF8Query : kAugQuery));
   FusedLaunch f{};
   f.nq = nq;
   f.nb = (int)v.n;

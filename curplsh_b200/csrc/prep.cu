@@ -97,10 +97,13 @@ __device__ __forceinline__ void prep_row(const float* __restrict__ x, long long 
   float inv = 1.f;
   if (f8) {
     m = warp_max(m);
-    // an all-zero row gets scale 0 (its codes are 0 whatever the scale)
-    const float sc = fixed_scale > 0.f ? fixed_scale : m / kE4M3Max;
+    // an all-zero row gets scale 0 (its codes are 0 whatever the scale); a
+    // zero query row with a norm tail gets 1, so its tail 1/s_q is finite
+    float sc = fixed_scale > 0.f ? fixed_scale : m / kE4M3Max;
+    const bool q_tail = aug == kAugF8Query;
+    if (q_tail && !(sc > 0.f)) sc = 1.f;
     inv = sc > 0.f ? 1.f / sc : 0.f;
-    if (scale && lane == 0) scale[r] = m > 0.f ? sc : 0.f;
+    if (scale && lane == 0) scale[r] = (m > 0.f || q_tail) ? sc : 0.f;
   }
   if (vec4) {
     const float4* row4 = reinterpret_cast<const float4*>(row);
@@ -167,6 +170,27 @@ __device__ __forceinline__ void prep_row(const float* __restrict__ x, long long 
         const float v = i < d ? row[i] : 0.f;
         f8[r * ld8 + i] = to_e4m3(v * inv);
       }
+  }
+  if (f8 && (aug == kAugF8Query || aug == kAugF8Database)) {
+    // the BF16 norm tail at byte t8 (a 32-byte K step of the last 128-byte
+    // chunk): a_h b_h + a_h b_l + a_l b_h = a b to ~2^-16 relative
+    const long long t8 = fp8_tail_offset(d, ld8);
+    if (t8 > 0) {
+      __syncwarp();  // after the zero fill above, which covers these bytes
+      float v = 0.f;
+      if (aug == kAugF8Query)
+        v = inv;  // 1 / s_q
+      else if (fixed_scale > 0.f)
+        v = -0.5f * s / fixed_scale;  // -||x||^2 / (2 s)
+      const float vh = __bfloat162float(__float2bfloat16_rn(v));
+      const float vl = v - vh;  // exact
+      float e = 0.f;
+      if (aug == kAugF8Query)
+        e = lane < 2 ? vh : (lane == 2 ? vl : 0.f);
+      else
+        e = lane == 1 ? vl : (lane == 0 || lane == 2 ? vh : 0.f);
+      if (lane < 16) reinterpret_cast<__nv_bfloat16*>(f8 + r * ld8 + t8)[lane] = __float2bfloat16_rn(e);
+    }
   }
   if (lo_nonzero && __any_sync(0xffffffffu, lo_any) && lane == 0) atomicOr(lo_nonzero, 1u);
 }

@@ -112,6 +112,8 @@ SHAPES = [
     (3000, 130, 100, 33),  # d not a multiple of 8
     (4097, 300, 128, 100),
     (2000, 50, 256, 1),
+    (2500, 150, 160, 20),  # FP8 norm tail in the second K chunk (byte 160)
+    (1200, 90, 200, 12),   # FP8 norm tail at byte 224 (the last step of chunk 2)
     (1500, 64, 512, 200),
     (600, 10, 1000, 5),    # very high d: query chunks stream with the database
 ]
