@@ -486,6 +486,16 @@ def run_batched(cb, synth, args, world, rank, local, res, peaks):
         return max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
 
     ms_graph = timed(lambda: batch.run(stream=stream, wait=False))
+    # the other form's graph over the same items: its replay time, and its
+    # results must equal this form's (both rerank exactly)
+    other = 1 - precision if precision in (0, 1) else 1
+    alt_batch = cb.SearchBatch(items, precision=other)
+    ref_out = [(it[3].clone(), it[4].clone()) for it in items]
+    alt_batch.run(stream=stream)
+    alt_same = all(torch.equal(a, it[3]) and torch.equal(b, it[4]) for (a, b), it in zip(ref_out, items))
+    ms_alt = timed(lambda: alt_batch.run(stream=stream, wait=False))
+    alt_batch.close()
+    del ref_out
 
     def one_by_one():
         for ix, q, k, oi, od in items:
@@ -531,6 +541,8 @@ def run_batched(cb, synth, args, world, rank, local, res, peaks):
                    "k_values": sorted({b[2] for b in batches}), "form": FORMS[precision],
                    "seed": synth.SEEDS["batched_uneven"], "l2": "databases (3.1 GB) larger than L2"},
         "one_by_one": {"queries_per_s": total_q * world / (ms_loop / 1e3), "ms_per_step": ms_loop},
+        "other_form": {"form": FORMS[other], "ms_per_step": ms_alt, "queries_per_s": total_q * world / (ms_alt / 1e3),
+                       "identical_results": alt_same},
         "batch_speedup": ms_loop / ms_graph,
         "identical_to_alone": mismatches == 0, "items_differing": mismatches,
         "recall_at_k_min_sampled": recall_min, "max_rel_dist_err_sampled": err_max,
@@ -746,7 +758,8 @@ def main():
     ap.add_argument("--serve-rates", type=lambda v: [int(x) for x in v.split(",")], default=[1000, 5000, 20000, 50000],
                     help="serving workload: offered query rates (queries/s)")
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="serving workload: seconds per rate")
-    ap.add_argument("--batch-form", type=int, default=1, help="precision form of the batched workload")
+    ap.add_argument("--batch-form", type=int, default=0,
+                    help="precision form of the batched workload (the other of 0 / 1 is timed beside it)")
     ap.add_argument("--tune", action="store_true", help="batched workload: autotune its buckets first")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -544,17 +544,20 @@ def get_coarse_check() -> bool:
     return bool(v.value)
 
 
-def set_cta_pairs(enabled: bool) -> None:
-    """Process-wide switch of CTA pairs: fused passes over >= 4 query blocks run
-    as clusters of two CTAs sharing one 256-row tensor-core MMA (off by default;
-    results do not depend on it)."""
-    _check(_lib.curplsh_set_cta_pairs(1 if enabled else 0))
+def set_cta_pairs(mode) -> None:
+    """Process-wide CTA pairs mode: fused passes over >= 4 query blocks run as
+    clusters of two CTAs sharing one 256-row tensor-core MMA.  True: every such
+    pass; False: none; "auto" (the default): BF16 passes with d >= 320 and
+    FP32-exact passes with d >= 192.  Results do not depend on it."""
+    v = 2 if mode == "auto" else (1 if mode else 0)
+    _check(_lib.curplsh_set_cta_pairs(v))
 
 
-def get_cta_pairs() -> bool:
+def get_cta_pairs():
+    """True, False or "auto" (see set_cta_pairs)."""
     v = ctypes.c_int(0)
     _check(_lib.curplsh_get_cta_pairs(ctypes.byref(v)))
-    return bool(v.value)
+    return "auto" if v.value == 2 else bool(v.value)
 
 
 def set_dual_blocks(enabled: bool) -> None:

@@ -1218,6 +1218,7 @@ int curplsh_get_coarse_check(int* enabled) {
 }
 
 int curplsh_set_cta_pairs(int enabled) {
+  if (enabled < 0 || enabled > kPairsAuto) return set_error(CURPLSH_ERR_INVALID_ARG, "CTA pairs mode must be 0, 1 or 2");
   set_cta_pairs(enabled);
   return CURPLSH_OK;
 }

@@ -1254,11 +1254,21 @@ cudaError_t launch_form_any(const FusedItemSpec* specs, const FusedItemPlan* pla
 #define CURPLSH_DUAL_DEFAULT 1
 #endif
 namespace {
-std::atomic<int> g_cta_pairs{0};
+std::atomic<int> g_cta_pairs{kPairsAuto};
 std::atomic<int> g_dual{CURPLSH_DUAL_DEFAULT};
+// Automatic CTA pairs: from these dimensions on, the MMAs of a tile are heavy
+// enough that halving each SM's database bytes per query pays.  Measured on
+// 10^6 N(0,1) BF16-valued rows, 4,096 queries (k = 10) and 2,048 (k = 100),
+// single CTAs -> pairs: BF16 d = 128 2.33 -> 2.93 ms, 256 3.15 -> 3.44, 320
+// 3.59 -> 3.48, 384 4.67 -> 3.83, 512 5.98 -> 4.54; FP32-exact d = 128 3.44 ->
+// 3.43, 192 4.75 -> 4.36, 256 6.10 -> 5.55, 512 11.5 -> 9.9 (identical results).
+constexpr int kPairMinDimBF16 = 320;
+constexpr int kPairMinDimExact = 192;
 }  // namespace
 
-void set_cta_pairs(int on) { g_cta_pairs.store(on ? 1 : 0, std::memory_order_relaxed); }
+void set_cta_pairs(int mode) {
+  g_cta_pairs.store(mode == kPairsAuto ? kPairsAuto : (mode ? 1 : 0), std::memory_order_relaxed);
+}
 int get_cta_pairs() { return g_cta_pairs.load(std::memory_order_relaxed); }
 void set_dual_blocks(int on) { g_dual.store(on ? 1 : 0, std::memory_order_relaxed); }
 int get_dual_blocks() { return g_dual.load(std::memory_order_relaxed); }
@@ -1282,7 +1292,11 @@ void plan_fused_batch(const FusedItemSpec* specs, int n, int max_ctas, FusedItem
   // (sphere 39.6 -> 37.7 ms); the BF16 pass got slower (3.50 -> 4.52 ms on the
   // integer mixture: twice the MMA instructions and shared-memory A reads)
   const int dual = (grouped && dual_fits && get_dual_blocks() && form == kFormFP8) ? 1 : 0;
-  const int pair = (!dual && grouped && get_cta_pairs() && max_ctas >= 2) ? 1 : 0;
+  const int pm = get_cta_pairs();
+  const int d0 = n > 0 ? specs[0].d : 0;
+  const bool want_pair = pm == 1 || (pm == kPairsAuto && ((form == kFormBF16 && d0 >= kPairMinDimBF16) ||
+                                                          (form == kFormExact && d0 >= kPairMinDimExact)));
+  const int pair = (!dual && grouped && want_pair && max_ctas >= 2) ? 1 : 0;
   const int rows = kBM << (pair | dual);
   const int tile_rows = dual ? kBN / 2 : kBN;
   long long total = 0;

@@ -121,7 +121,10 @@ struct FusedBatchPlan {
   int dual = 0;  // 1: each CTA takes query groups of two blocks and 128-row database tiles
 };
 // CTA pairs on (1) or off (0, default) for the plans made after the call.
-void set_cta_pairs(int on);
+// CTA pairs: 0 off, 1 on (every grouped pass), kPairsAuto (the default): on
+// for BF16 passes with d >= 320 and FP32-exact passes with d >= 192
+constexpr int kPairsAuto = 2;
+void set_cta_pairs(int mode);
 int get_cta_pairs();
 // Dual query blocks (BF16 / FP8) on or off for the plans made after the call.
 void set_dual_blocks(int on);

@@ -326,11 +326,14 @@ int curplsh_index_get_fallback_count(curplsh_index* index, int64_t* count);
  * it returns synchronised even with device buffers.  Process-wide; on (1) by default. */
 int curplsh_set_coarse_check(int enabled);
 int curplsh_get_coarse_check(int* enabled);
-/* CTA pairs (engine-specific, no counterpart in cuRPLSH; off by default): with it on, a fused
- * pass over at least four 128-query blocks runs as clusters of two CTAs, each pair sharing one
- * 256-row tensor-core MMA (tcgen05 cta_group::2) over two query blocks, so every database tile
- * crosses from L2 once per 256 queries instead of once per 128.  Results do not depend on it.
- * Applies to searches, batches and servers planned after the call.  Process-wide. */
+/* CTA pairs (engine-specific, no counterpart in cuRPLSH): a fused pass over at least four
+ * 128-query blocks runs as clusters of two CTAs, each pair sharing one 256-row tensor-core MMA
+ * (tcgen05 cta_group::2) over two query blocks, so every database tile crosses from L2 once per
+ * 256 queries instead of once per 128.  0 = off, 1 = on for every such pass, 2 = automatic (the
+ * default): on for BF16 passes with d >= 320 and FP32-exact passes with d >= 192, where the
+ * tensor work per tile is heavy enough for the halved tile bytes to pay (BF16 at d = 512: 5.98 ->
+ * 4.54 ms for 4,096 queries over 10^6 rows; at d = 128 pairs are slower).  Results do not depend
+ * on it.  Applies to searches, batches and servers planned after the call.  Process-wide. */
 int curplsh_set_cta_pairs(int enabled);
 int curplsh_get_cta_pairs(int* enabled);
 /* Dual query blocks (engine-specific, no counterpart in cuRPLSH; on by default): an FP8 fused

@@ -44,6 +44,8 @@ def test_switch_round_trips(env):
     assert cb.get_cta_pairs() is False
     cb.set_cta_pairs(True)
     assert cb.get_cta_pairs() is True
+    cb.set_cta_pairs("auto")
+    assert cb.get_cta_pairs() == "auto"
 
 
 # (rows, queries, dim, k): 8 query blocks; 17 blocks (the last group of two is
@@ -97,3 +99,22 @@ def test_pairs_in_the_batch_graph(env):
     batch.close()
     for ix, _ in dbs:
         ix.close()
+
+
+@pytest.mark.parametrize("form,d", [(1, 384), (0, 256)])
+def test_automatic_pairs_with_estimate(env, form, d):
+    """The automatic mode pairs BF16 passes from d = 320 and FP32-exact passes
+    from d = 192; with 70,000 rows the sampled bound estimate runs as well.
+    Results equal the single-CTA pass and the oracle."""
+    cb, res = env
+    rng = np.random.default_rng(31 + d)
+    n, nq, k = 70000, 1024, 10
+    base = _bf16_values(rng, (n, d))
+    queries = _bf16_values(rng, (nq, d))
+    d1, i1 = _search(cb, res, base, queries, k, form, pairs=False)
+    d2, i2 = _search(cb, res, base, queries, k, form, pairs="auto")
+    np.testing.assert_array_equal(i1, i2)
+    np.testing.assert_array_equal(d1, d2)
+    sub = np.arange(0, nq, 16)
+    rd, ri = oracle.knn(base, queries[sub], k + 1)
+    assert_knn_matches(base, queries[sub], d2[sub], i2[sub], rd, ri)
