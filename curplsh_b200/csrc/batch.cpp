@@ -8,7 +8,8 @@
 // (multi_plan.h) -- requests against one index with one (form, k') share
 // query blocks, one prep / fused / merge chain per (form, d) group -- with the
 // groups as parallel branches of the graph; each fused launch asks for every
-// SM, so a group's tail overlaps the next group's start.
+// SM, so a group's tail overlaps the next group's start; items too small to
+// spread over many CTAs of a combined launch get launches of their own.
 // Run: one cudaGraphLaunch.
 #include <cuda_runtime.h>
 

@@ -12,6 +12,13 @@
 namespace curplsh_b200 {
 namespace {
 
+// An item whose tiles would span fewer CTA ranges than this in its group's
+// combined launch gets a launch of its own.
+#ifndef CURPLSH_SOLO_CTAS
+#define CURPLSH_SOLO_CTAS 16
+#endif
+constexpr long long kSoloCtas = CURPLSH_SOLO_CTAS;
+
 int fail(int code, const char* fmt, ...) {
   char buf[512];
   va_list ap;
@@ -113,9 +120,30 @@ int MultiPlan::build(const curplsh_batch_item* items, int n, const std::vector<c
     // earlier group releases, while a static split of the SMs by tile count
     // would leave the groups whose tiles are dearer (larger d, larger k') as
     // the long pole.
+    //
+    // A launch splits its flattened (item, query block, tile) space into equal
+    // contiguous CTA ranges by tile count, so an item with few tiles lands on
+    // one or two CTAs; when its tiles are dear (a large k' against a small
+    // database, where every row survives) those CTAs become the launch's tail.
+    // An item whose work would span fewer than kSoloCtas CTA ranges of the
+    // combined launch therefore gets a launch of its own (spread over every
+    // SM); the larger items share one.
+    long long work_all = 0;
+    auto work_of = [&](int fi) {
+      const FItem& x = fitems_[fi];
+      return (long long)((x.nq + kBM - 1) / kBM) * ((views[x.slot].n + kBN - 1) / kBN);
+    };
+    for (int fi : G.fitems) work_all += work_of(fi);
+    const long long w_comb = std::max<long long>(1, (work_all + num_sms - 1) / num_sms);
     FLaunch L;
     for (int fi : G.fitems) {
       if (views[fitems_[fi].slot].n == 0) continue;
+      if (work_of(fi) < kSoloCtas * w_comb) {
+        FLaunch S;
+        S.fitems.push_back(fi);
+        G.launches.push_back(S);
+        continue;
+      }
       if ((int)L.fitems.size() == kFusedMaxItems) {
         G.launches.push_back(L);
         L.fitems.clear();
