@@ -666,6 +666,12 @@ def _serving_measure(cb, synth, args, rank, local, res, oracle, dev):
             sizes = request_sizes(count)
             gaps = rng.exponential(1.0 / mean_req, size=count)
             arrivals = np.cumsum(gaps) - gaps[0]
+            # half a second of the same load first, not measured: the rate is
+            # measured in its steady state, not in the transition from the
+            # previous (heavier) load
+            wcount = int(max(20, mean_req * 0.5))
+            wgaps = rng.exponential(1.0 / mean_req, size=wcount)
+            run_load(srv, request_sizes(wcount), list(np.cumsum(wgaps) - wgaps[0]))
             # a slower sampler with a longer settle: each nvidia-smi query takes
             # driver locks that a latency measurement would otherwise see
             sampler = ClockSampler(local, interval_ms=200, settle_s=1.0)
