@@ -299,21 +299,18 @@ __device__ __forceinline__ uint32_t shl1_sign(uint32_t acc, uint32_t t) {
   asm("shf.l.wrap.b32 %0, %1, %2, 1;" : "=r"(r) : "r"(t), "r"(acc));
   return r;
 }
-// Length of the funnel-shift chains that gather a survivor mask's sign bits:
-// two chains of 16 and one join per 32 columns (eight of 4 and seven joins
-// measured 3 % slower on the BF16 and FP8 passes: fewer instructions beat the
-// extra chain parallelism at two epilogue warps per sub-partition).
-#ifndef CURPLSH_MASK_CHAIN
-#define CURPLSH_MASK_CHAIN 16
-#endif
 // bit j set iff km dv[j] < u, computed exactly (one rounding of km dv[j] - u
-// keeps its sign); u = next_above(thr) makes it km dv[j] <= thr for km = 1
+// keeps its sign); u = next_above(thr) makes it km dv[j] <= thr for km = 1.
+// The sign bits are gathered by 32 / L funnel-shift chains of length L and
+// joined: fewer instructions beat the extra chain parallelism at two epilogue
+// warps per sub-partition (chains of 4 -> 16: BF16 pass 3.48 -> 3.37 ms; the
+// FP8 pass gains again from 16 -> 32, 30.1 -> 28.1 ms, BF16 loses 1 %).
+template <int L>
 __device__ __forceinline__ uint32_t survive_mask32(const float (&dv)[32], float km, float u) {
   float t[32];
 #pragma unroll
   for (int i = 0; i < 16; ++i) fma2_f32(t[2 * i], t[2 * i + 1], dv[2 * i], dv[2 * i + 1], km, km, -u, -u);
   // 32 / L independent chains of L funnel shifts, then their L-bit pieces joined
-  constexpr int L = CURPLSH_MASK_CHAIN;
   uint32_t c[32 / L];
 #pragma unroll
   for (int p = 0; p < 32 / L; ++p) {
@@ -927,8 +924,9 @@ __global__ void __launch_bounds__(threads_for(MINIMA), 1) fused_knn_kernel(const
             ma = survive_mask32_cmp(da, thr);
             mb = survive_mask32_cmp(db, thr);
           } else {
-            ma = survive_mask32(da, km, thr_up);
-            mb = survive_mask32(db, km, thr_up);
+            constexpr int kChain = Tr::kFP8 ? 32 : 16;
+            ma = survive_mask32<kChain>(da, km, thr_up);
+            mb = survive_mask32<kChain>(db, km, thr_up);
           }
           if (!valid) ma = mb = 0u;
           // database rows beyond nb (padding of the last tile) never survive
